@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Benchmark of the batched training forward (srkTrainingForward drop-in).
+
+Workload (one step): R_b = dx^2 (conv(E_b,Gx) dE_b/dx + conv(E_b,Gy) dE_b/dy)
+for B = 5000 images of N = 512 (E = I, KW = 121, W = 392, dx = 4 nm, Green's
+tensor gamma = 1/30 nm, R_w = erosion*dx), fp32, inputs already resident in
+HBM (5.2 GB > L2, so no flush is needed between steps).  Inputs are seeded
+Gaussian random fields (correlation length 8 px, min-max scaled to [0,1]).
+
+Multi-GPU: one process per GPU, each rank runs its own B images (weak
+scaling, no data-path collective); the step time is the max over ranks.
+
+Extra keys: roofline (HBM, algorithmic (N^2+W^2)*4 bytes per image),
+cpu_baseline (FP64 oracle on the host cores, rank 0 at N=1), e2e (host
+buffers through the public API, copies inside the timed region), clocks,
+gpu_launches, ops (per-operator throughput of the OaS derivatives).
+
+--impl reference times the reference's CPU path restated by the oracle on
+all host cores (the reference's own CPU code does not build on its own), and
+adds the reference's own cuFFT srkTrainingForward built from its sources as
+"gpu_reference".
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--B", type=int, default=5000)
+    p.add_argument("--N", type=int, default=512)
+    p.add_argument("--KW", type=int, default=121)
+    p.add_argument("--dx", type=float, default=4.0)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-ops", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(N, KW, B):
+    """dram bytes per launch sequence from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    key = "N=%d KW=%d" % (N, KW)
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith(key) and "bytes_per_image=" in line:
+                per_img = float(line.split("bytes_per_image=")[1].split()[0])
+                return per_img * B
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def grf_batch(torch, B, N, seed0, ell=8.0, chunk=250):
+    """Seeded Gaussian random fields on the device, col-major [B][N][N]."""
+    out = torch.empty((B, N, N), device="cuda", dtype=torch.float32)
+    k = torch.fft.fftfreq(N, device="cuda", dtype=torch.float64)
+    H = torch.exp(-2.0 * (torch.pi ** 2) * ell ** 2 * (k[:, None] ** 2 + k[None, :] ** 2))
+    for b0 in range(0, B, chunk):
+        b1 = min(B, b0 + chunk)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed0 + b0)
+        w = torch.randn((b1 - b0, N, N), device="cuda", dtype=torch.float64, generator=gen)
+        x = torch.fft.ifft2(torch.fft.fft2(w) * H).real
+        mn = x.amin(dim=(1, 2), keepdim=True)
+        mx = x.amax(dim=(1, 2), keepdim=True)
+        out[b0:b1] = ((x - mn) / (mx - mn)).float()
+    return out
+
+
+def make_spectra(torch, srk, KW, N, dx):
+    e = (KW - 1) // 2
+    Kx = torch.zeros((KW, KW), device="cuda")
+    Ky = torch.zeros_like(Kx)
+    srk.green_tensor(Kx, Ky, 1.0 / 30.0, e * dx, dx)
+    GX = torch.zeros((N, N // 2 + 1), dtype=torch.complex64, device="cuda")
+    GY = torch.zeros_like(GX)
+    srk.srkPrecomputeKernelFreq(Kx, KW, KW, N, GX)
+    srk.srkPrecomputeKernelFreq(Ky, KW, KW, N, GY)
+    torch.cuda.synchronize()
+    return Kx, Ky, GX, GY
+
+
+def cpu_oracle_rate(N, KW, dx, seconds, nthreads):
+    """Images/s of the FP64 oracle forward (direct valid convolution) on the host."""
+    import numpy as np
+    from oracle import oracle as O
+    e = (KW - 1) // 2
+    Kx, Ky = O.make_kernel(KW, dx, 1.0 / 30.0, e * dx)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        E = O.grf(N, 8.0, 1000 + n).astype(np.float64)
+        O.forward(E, E, Kx, Ky, e, dx, nthreads=nthreads)
+        n += 1
+        el = time.perf_counter() - t0
+        if (el >= seconds and n >= 2) or n >= 200:
+            break
+    return n / el, n, el
+
+
+def time_steps(torch, fn, steps, warmup, dist):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s = torch.cuda.Event(enable_timing=True)
+    t = torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        fn()
+    t.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(t) / steps
+    if dist:
+        dist.barrier()
+    return ms
+
+
+def max_over_ranks(torch, dist, x):
+    if not dist:
+        return x
+    v = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+    return float(v.item())
+
+
+def e2e_pipeline(torch, srk, plan, GX, GY, N, W, e, dx, B, steps, warmup, dist, chunk=500):
+    """Host-buffer end to end: pinned host E -> device, forward, device -> pinned
+    host R, chunked over three streams so copies overlap compute."""
+    Eh = torch.empty((B, N, N), dtype=torch.float32).pin_memory()
+    Eh.uniform_()
+    Rh = torch.empty((B, W, W), dtype=torch.float32).pin_memory()
+    nslot = 3
+    dE = [torch.empty((chunk, N, N), device="cuda") for _ in range(nslot)]
+    dR = [torch.empty((chunk, W, W), device="cuda") for _ in range(nslot)]
+    s_in, s_cmp, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(nslot)]
+    ev_cmp = [torch.cuda.Event() for _ in range(nslot)]
+    ev_out = [torch.cuda.Event() for _ in range(nslot)]
+    cur = torch.cuda.current_stream()
+
+    def step():
+        start = torch.cuda.Event()
+        start.record(cur)
+        for st in (s_in, s_cmp, s_out):
+            st.wait_event(start)
+        for i, b0 in enumerate(range(0, B, chunk)):
+            b1 = min(B, b0 + chunk)
+            k = i % nslot
+            if i >= nslot:
+                s_in.wait_event(ev_out[k])       # slot free again
+            with torch.cuda.stream(s_in):
+                dE[k][: b1 - b0].copy_(Eh[b0:b1], non_blocking=True)
+                ev_in[k].record(s_in)
+            s_cmp.wait_event(ev_in[k])
+            srk.srkTrainingForward(dE[k], dE[k], GX, GY, N, W, e, dx, b1 - b0, s_cmp, dR[k], plan)
+            ev_cmp[k].record(s_cmp)
+            s_out.wait_event(ev_cmp[k])
+            with torch.cuda.stream(s_out):
+                Rh[b0:b1].copy_(dR[k][: b1 - b0], non_blocking=True)
+                ev_out[k].record(s_out)
+        for st in (s_in, s_cmp, s_out):
+            end = torch.cuda.Event()
+            end.record(st)
+            cur.wait_event(end)
+
+    ms = time_steps(torch, step, steps, warmup, dist)
+    return ms, B * N * N * 4, B * W * W * 4
+
+
+def run_ours(a):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist = td
+    import shrinkage_full_tests_b200 as srk
+
+    N, KW, B, dx = a.N, a.KW, a.B, a.dx
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
+    E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17)
+    R = torch.empty((B, W, W), device="cuda")
+    plan = srk.SrkPlan(N, W, e, dx, B)
+    info = plan.info()
+    step = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
+    step()
+    torch.cuda.synchronize()
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms = time_steps(torch, step, a.steps, a.warmup, dist)
+    clocks = clk.stop()
+    ms = max_over_ranks(torch, dist, ms)
+    imgs_per_s = world * B / (ms * 1e-3)
+    mpix = world * B * W * W / (ms * 1e-3) / 1e6
+
+    nwt = (B * info["tiles"] ** 2 + 1) // 2
+    launches_per_step = 3 * ((nwt + info["chunk_wt"] - 1) // info["chunk_wt"])
+    peak, peak_kind = measured_peaks()
+    alg_bytes = B * (N * N + W * W) * 4
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    traffic = profiled_traffic(N, KW, B)
+
+    e2e = None
+    if not a.no_e2e:
+        ms_e2e, h2d, d2h = e2e_pipeline(torch, srk, plan, GX, GY, N, W, e, dx, B, max(2, a.steps // 2),
+                                        1, dist)
+        ms_e2e = max_over_ranks(torch, dist, ms_e2e)
+        e2e = {"value": world * B / (ms_e2e * 1e-3), "unit": "img/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e, "pipeline": "3 streams, 500-image chunks"}
+
+    ops = None
+    if not a.no_ops and world == 1:
+        ops = ops_throughput(torch, srk)
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        nth = os.cpu_count() or 1
+        rate, n, el = cpu_oracle_rate(N, KW, dx, a.cpu_seconds, nth)
+        cpu = {"value": rate, "unit": "img/s", "cores": nth, "kind": "port",
+               "sample": "%d images of N=%d KW=%d, FP64 direct valid convolution (oracle), %.1f s" % (n, N, KW, el)}
+
+    if dist:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": "srkTrainingForward images/s (B=5000 per GPU, N=512, KW=121)",
+            "value": imgs_per_s, "unit": "img/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: seeded Gaussian random fields (ell=8 px, [0,1]), device-resident",
+            "config": {"workload": "srkTrainingForward B=%d N=%d KW=%d W=%d dx=%g nm gamma=1/30 nm" % (B, N, KW, W, dx),
+                       "B_per_gpu": B, "N": N, "KW": KW, "W": W, "tile_M": info["tile_M"],
+                       "l2": "inputs (%.1f GB/GPU) larger than L2; no flush" % (B * N * N * 4 / 1e9),
+                       "parallelism": "dp%d (batch shards, no collective)" % world},
+            "output_mpix_per_s": mpix,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": "srkTrainingForward launch sequence (P1+P2+P3 per chunk)",
+                         "algorithmic_bytes_per_step": alg_bytes},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": launches_per_step * a.steps,
+            "ops": ops,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
+    """Output Mpix/s of each OaS operator on one N x N image (one GPU)."""
+    import numpy as np
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    _, _, GX, GY = make_spectra(torch, srk, KW, 1024, 1.0)
+    f, g = grf_batch(torch, 2, N, 77)
+    df, dg = (1e-2 * torch.randn((2, N, N), device="cuda")).unbind(0)
+    lam, dlam = torch.randn((2, W, W), device="cuda").unbind(0)
+    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=1024)
+    R = torch.empty((W, W), device="cuda")
+    ux, uy = torch.empty_like(R), torch.empty_like(R)
+    o1, o2 = torch.empty((N, N), device="cuda"), torch.empty((N, N), device="cuda")
+    runs = {
+        "forward": lambda: srk.srkForwardOaS(g, f, GX, GY, N, W, e, 1.0, None, R, plan, ux, uy),
+        "adjoint": lambda: srk.adjointSRK(lam, ux, uy, f, GX, GY, N, W, e, 1.0, None, o1, o2, plan),
+        "tangent": lambda: srk.shrinkageTangentOaS(f, g, df, dg, GX, GY, N, W, e, 1.0, None, R, plan),
+        "tangent_adjoint": lambda: srk.shrinkageTangentAdjointOaS(f, g, df, dg, lam, dlam, GX, GY, N, W, e, 1.0,
+                                                                   None, o1, o2, plan),
+    }
+    out = {"config": "N=%d KW=%d B=1 fp32 tile_M=%d" % (N, KW, plan.info()["tile_M"])}
+    alg = {"forward": 2 * N * N + W * W, "adjoint": 3 * W * W + N * N + 2 * N * N,
+           "tangent": 4 * N * N + W * W, "tangent_adjoint": 6 * N * N + 2 * W * W}
+    peak, _ = measured_peaks()
+    for k, fn in runs.items():
+        ms = time_steps(torch, fn, reps, 2, None)
+        px = W * W if k in ("forward", "tangent") else N * N
+        out[k] = {"ms": ms, "out_mpix_per_s": px / (ms * 1e-3) / 1e6,
+                  "hbm_frac": alg[k] * 4 / (ms * 1e-3) / 1e9 / peak}
+    return out
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    N, KW, B, dx = a.N, a.KW, a.B, a.dx
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    nth = os.cpu_count() or 1
+    import numpy as np
+    from oracle import oracle as O
+    Kx, Ky = O.make_kernel(KW, dx, 1.0 / 30.0, e * dx)
+    sample = 4  # images per step
+    imgs = [O.grf(N, 8.0, 2000 + i).astype(np.float64) for i in range(sample)]
+
+    def step():
+        for E in imgs:
+            O.forward(E, E, Kx, Ky, e, dx, nthreads=nth)
+
+    for _ in range(a.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    el = (time.perf_counter() - t0) / a.steps
+    rate = sample / el
+    line = {
+        "impl": "reference", "metric": "srkTrainingForward images/s (B=5000 per GPU, N=512, KW=121)",
+        "value": rate, "unit": "img/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": el * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: seeded Gaussian random fields (ell=8 px, [0,1])",
+        "config": {"workload": "srkTrainingForward B=%d N=%d KW=%d W=%d dx=%g nm gamma=1/30 nm" % (B, N, KW, W, dx),
+                   "sample_per_step": "%d images (bounded sample of the B=%d workload)" % (sample, B)},
+        "cpu_baseline": {"value": rate, "unit": "img/s", "cores": nth, "kind": "port",
+                         "sample": "%d images per step, FP64 direct valid convolution (oracle restating "
+                                   "cpu_conv_valid, adjoint/main_adjoint.cu:70-90)" % sample},
+        "e2e": {"value": rate, "unit": "img/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line["gpu_reference"] = gpu_reference(a)
+    print(json.dumps(line))
+
+
+def gpu_reference(a):
+    """The reference's own cuFFT srkTrainingForward (built from its sources into
+    oracle/_ref) on this GPU, same workload; None if unavailable."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from tests.gpu_util import ref_gpu
+        L = ref_gpu()
+        if L is None:
+            return {"unavailable": "oracle/_ref/libref_gpu.so not built"}
+        import shrinkage_full_tests_b200 as srk
+        N, KW, B, dx = a.N, a.KW, a.B, a.dx
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
+        E = grf_batch(torch, B, N, 17)
+        R = torch.empty((B, W, W), device="cuda")
+        free0 = torch.cuda.mem_get_info()[0]
+        st = torch.cuda.current_stream().cuda_stream
+        ws = L.ref_train_ws_create(N, B, st)
+        ws_bytes = free0 - torch.cuda.mem_get_info()[0]
+        fn = lambda: L.ref_train_forward(E.data_ptr(), E.data_ptr(), GX.data_ptr(), GY.data_ptr(), N, W, e, dx, B,
+                                         st, R.data_ptr(), ws)
+        ms = time_steps(torch, fn, max(2, a.steps), 1, None)
+        L.ref_train_ws_destroy(ws, st)
+        return {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "workspace_bytes": ws_bytes,
+                "what": "reference srkTrainingForward (cuFFT) compiled for sm_100a from its sources"}
+    except Exception as ex:  # the CPU line must still print
+        return {"unavailable": "%s" % ex}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,159 @@
+/*
+ * srk_b200.h — C ABI of the B200 (sm_100a) resist-shrinkage operator library.
+ *
+ *   h = c * ( conv(Gx, g) * df/dx + conv(Gy, g) * df/dy )      (valid, W = N - 2*erosion)
+ *
+ * Every buffer is a device pointer; every image is column-major
+ * buf[col*H + row] with batch stride N*N (inputs) or W*W (outputs).  Kernel
+ * spectra are accepted in the reference's layout: the unnormalised R2C
+ * spectrum of the fftshifted, column-major M x M padded kernel,
+ * freq[kx*(M/2+1) + ky] (complex64 = two floats), M = the plan's spectra_M.
+ *
+ * All entry points are stream-ordered and asynchronous (no host sync); they
+ * return a status instead of aborting.  The *_sync variants add a
+ * cudaStreamSynchronize, like the reference's operators.
+ *
+ * The plan (srk_plan) replaces the reference's workspace structs
+ * (SrkTrainWorkspace, SrkConvWorkspace, SrkAdjWorkspace, SrkTanWorkspace,
+ * SrkTanAdjWorkspace): it owns the scratch, the re-laid-out kernel spectra
+ * and the tile configuration.  A plan is bound to one device and must not be
+ * used from two host threads at once.
+ */
+#ifndef SRK_B200_H
+#define SRK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* srk_stream_t; /* == cudaStream_t */
+typedef struct srk_plan_s* srk_plan;
+
+typedef enum srk_status {
+  SRK_OK = 0,
+  SRK_ERR_INVALID_ARG = 1, /* bad size / null pointer / mismatch with the plan */
+  SRK_ERR_UNSUPPORTED = 2, /* valid request this build cannot serve (e.g. tile too small) */
+  SRK_ERR_ALLOC = 3,       /* device allocation failed */
+  SRK_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  SRK_ERR_CUDA = 5         /* a CUDA runtime call failed */
+} srk_status;
+
+typedef enum srk_dtype { SRK_F32 = 0, SRK_F16 = 1, SRK_BF16 = 2 } srk_dtype;
+
+/* How the adjoint with respect to the convolved field applies the kernel.
+ * SRK_ADJ_REFERENCE multiplies by the stored spectrum, i.e. convolves the
+ * cotangent with G exactly like adjointWrtE (adjoint/srk_adjoint.cuh:301-382).
+ * SRK_ADJ_TRUE multiplies by its conjugate, i.e. correlates with G, which is
+ * the exact adjoint of the forward convolution for any kernel.  The two agree
+ * for even kernels and differ by a sign for the odd Green's tensor. */
+typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_adj_convention;
+
+typedef struct srk_plan_info {
+  int N, W, erosion, B_max, spectra_M;
+  float dx;
+  int tile_M;       /* FFT tile size of the forward geometry */
+  int tile_stride;  /* valid outputs per tile per axis */
+  int tiles;        /* tiles per axis, forward geometry */
+  int tiles_adj;    /* tiles per axis, adjoint (full N x N output) geometry */
+  int chunk_wt;     /* work tiles per scratch chunk */
+  size_t scratch_bytes;
+  srk_dtype dtype;
+} srk_plan_info;
+
+/* ---- library ------------------------------------------------------------ */
+int srk_version(void);
+const char* srk_status_string(srk_status s);
+/* Message of the last failing call on this host thread ("" if none). */
+const char* srk_last_error(void);
+
+/* ---- plans ----------------------------------------------------------------
+ * N, W, erosion: image size, valid size, halo (W == N - 2*erosion).
+ * dx: pixel pitch (the convolution is scaled by dx^2).
+ * B_max: largest batch a call may pass.
+ * spectra_M: FFT size of the caller's spectra (N for srkTrainingForward,
+ *            the reference's M_TILE for the OaS operators).
+ * tile_M: 0 = choose automatically, else 128, 256 or 512.
+ * scratch_budget_bytes: 0 = default (1 GiB). */
+srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, int B_max, int spectra_M,
+                           srk_dtype dtype, int tile_M, size_t scratch_budget_bytes);
+srk_status srk_plan_destroy(srk_plan plan);
+srk_status srk_plan_get_info(srk_plan plan, srk_plan_info* info);
+srk_status srk_plan_set_adj_convention(srk_plan plan, srk_adj_convention conv);
+
+/* Import caller spectra (reference layout, size spectra_M).  Done implicitly
+ * by the operators whenever they see spectrum pointers different from the
+ * last imported ones; call it again after changing spectrum contents in
+ * place. */
+srk_status srk_plan_import_spectra(srk_plan plan, const void* d_Gx_freq, const void* d_Gy_freq,
+                                   srk_stream_t stream);
+/* Set the kernel from its spatial form: d_Kx, d_Ky column-major KW x KW
+ * floats, KW <= 2*erosion+1.  Spectra pointers passed to later calls may
+ * then be NULL. */
+srk_status srk_plan_set_kernel(srk_plan plan, const float* d_Kx, const float* d_Ky, int KW,
+                               srk_stream_t stream);
+
+/* ---- kernel generation (FP64 on the device) --------------------------------
+ * Green's tensor Gx = (gamma/2pi)(x/r)K1(gamma r)w(r), Gy likewise, radial
+ * Blackman window of radius R_w, zero at r = 0; x = (i - KW/2)*dx.
+ * Replaces make_kernel (training/main_cd_training.cu:40-77). */
+srk_status srk_green_tensor(float* d_Kx, float* d_Ky, int KW, double gamma, double R_w, double dx,
+                            srk_stream_t stream);
+/* Spectrum of a spatial kernel at size M in the reference layout, computed in
+ * FP64.  Replaces srkPrecomputeKernelFreq (srk_forward.cuh:154-203). */
+srk_status srk_precompute_kernel_freq(const float* d_K, int KW, int M, void* d_freq, srk_stream_t stream);
+
+/* ---- operators (reference parameter lists; the plan replaces `ws`) ------- */
+
+/* srkTrainingForward (training/srk_training_forward.cuh:175-241):
+ * R_b = dx^2 (conv(E_b,Gx) dI_b/dx + conv(E_b,Gy) dI_b/dy), b < B.
+ * d_E, d_I [B][N][N]; d_R [B][W][W]; spectra [N][N/2+1] (spectra_M == N). */
+srk_status srk_training_forward(const float* d_E, const float* d_I, const void* d_Gx_freq,
+                                const void* d_Gy_freq, int N, int W, int erosion, float dx, int B,
+                                srk_stream_t stream, float* d_R, srk_plan plan);
+srk_status srk_training_forward_sync(const float* d_E, const float* d_I, const void* d_Gx_freq,
+                                     const void* d_Gy_freq, int N, int W, int erosion, float dx, int B,
+                                     srk_stream_t stream, float* d_R, srk_plan plan);
+
+/* srkForwardOaS (srk_forward.cuh:468-501): one image; d_ux, d_uy optional
+ * [W][W] outputs of dx^2 conv(E,Gx), dx^2 conv(E,Gy) (may be NULL). */
+srk_status srk_forward_oas(const float* d_E, const float* d_I, const void* d_Gx_freq, const void* d_Gy_freq,
+                           int N, int W, int erosion, float dx, srk_stream_t stream, float* d_R,
+                           srk_plan plan, float* d_ux, float* d_uy);
+
+/* adjointSRK (adjoint/srk_adjoint.cuh:402-425): given v = dL/dR and the
+ * forward's ux, uy: dL/dI = Dx^T(ux v) + Dy^T(uy v), dL/dE = dx^2 (G (*) (v dI/dx) + ...)
+ * (kernel applied per the plan's convention).  d_dLdI, d_dLdE [N][N]. */
+srk_status srk_adjoint(const float* d_v, const float* d_ux, const float* d_uy, const float* d_I,
+                       const void* d_Gx_freq, const void* d_Gy_freq, int N, int W, int erosion, float dx,
+                       srk_stream_t stream, float* d_dLdI, float* d_dLdE, srk_plan plan);
+
+/* shrinkageTangentOaS (tan_tanadj/srk_tangent.cuh:111-151): JVP dh [W][W]. */
+srk_status srk_tangent(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                       const void* d_Gx_freq, const void* d_Gy_freq, int N, int W, int erosion, float dx,
+                       srk_stream_t stream, float* d_dh, srk_plan plan);
+
+/* shrinkageTangentAdjointOaS (tan_tanadj/srk_tangent_adjoint.cuh:105-159):
+ * d_dLam_f, d_dLam_g [N][N]. */
+srk_status srk_tangent_adjoint(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                               const float* d_lam_h, const float* d_dlam_h, const void* d_Gx_freq,
+                               const void* d_Gy_freq, int N, int W, int erosion, float dx,
+                               srk_stream_t stream, float* d_dLam_f, float* d_dLam_g, srk_plan plan);
+
+/* ---- save-for-backward contract (no reference counterpart of this exact
+ * signature; it recomputes conv(g,G) instead of taking ux, uy) ------------
+ * forward: h = srk_forward_oas with E = g, I = f, batched.
+ * vjp: (dL/df, dL/dg) from v = dL/dh and the saved f, g; B images. */
+srk_status srk_forward(const float* d_f, const float* d_g, int B, srk_stream_t stream, float* d_h,
+                       srk_plan plan);
+srk_status srk_vjp(const float* d_v, const float* d_f, const float* d_g, int B, srk_stream_t stream,
+                   float* d_dLdf, float* d_dLdg, srk_plan plan);
+srk_status srk_jvp(const float* d_f, const float* d_g, const float* d_df, const float* d_dg, int B,
+                   srk_stream_t stream, float* d_dh, srk_plan plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SRK_B200_H */

@@ -1,0 +1,215 @@
+"""FP64 CPU oracle for the resist-shrinkage operator — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and
+reference legs use this module, and only as the checker; the product
+(shrinkage_full_tests_b200) never imports it.
+
+Everything is column-major like the reference: an image array ``a`` of shape
+(N, N) here is indexed ``a[col, row]`` and its memory is buf[col*N + row].
+Kernels are (KW, KW) arrays indexed ``K[i, j]`` = column offset i - KW//2,
+row offset j - KW//2, i.e. the reference's K[i*KW + j].
+
+The C restatement (srk_oracle.c) cites the reference function each routine
+follows.  The reference's own generators (GpGenerator, generate_pattern) are
+available through oracle/_ref when the reference was compiled (oracle/build.py).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+_ref_host = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def nthreads_default():
+    return int(os.environ.get("SRK_ORACLE_THREADS", os.cpu_count() or 1))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(_HERE, "_build", "libsrk_oracle.so")
+        if not os.path.exists(path):
+            path = _build.build_oracle()
+        L = ctypes.CDLL(path)
+        i, d = ctypes.c_int, ctypes.c_double
+        L.oracle_conv_window.argtypes = [_dp, i, _dp, _dp, i, i, d, i, i, i, i, _dp, _dp, i]
+        L.oracle_forward_window.argtypes = [_dp, _dp, i, _dp, _dp, i, i, d, i, i, i, i, _dp, _dp, _dp, i]
+        L.oracle_adj_wrt_I.argtypes = [_dp, _dp, i, i, i, _dp]
+        L.oracle_adj_wrt_E.argtypes = [_dp, _dp, _dp, _dp, i, i, i, i, d, i, _dp, i]
+        L.oracle_tangent.argtypes = [_dp, _dp, _dp, _dp, _dp, _dp, i, i, i, i, d, _dp, i]
+        L.oracle_tangent_adjoint.argtypes = [_dp] * 8 + [i, i, i, i, d, i, _dp, _dp, i]
+        L.oracle_make_kernel.argtypes = [i, ctypes.c_float, ctypes.c_float, ctypes.c_float, _fp, _fp]
+        L.oracle_kernel_freq.argtypes = [_fp, i, i, _fp]
+        L.oracle_grad.argtypes = [_dp, i, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _cm(a):
+    """(N,N) [col,row] array -> its column-major memory is a C-contiguous copy."""
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def grad(I):
+    """Central differences (dI/dx along columns, dI/dy along rows), zero outside."""
+    I, pI = _d(I)
+    N = I.shape[0]
+    Ix = np.empty_like(I)
+    Iy = np.empty_like(I)
+    lib().oracle_grad(pI, N, Ix.ctypes.data_as(_dp), Iy.ctypes.data_as(_dp))
+    return Ix, Iy
+
+
+def conv_valid(E, Gx, Gy, erosion, dx, window=None, nthreads=None):
+    """(ux, uy) = dx^2 * valid conv of E with Gx, Gy on the output window
+    (ox0, oy0, wx, wy) (default: the whole W x W)."""
+    E, pE = _d(E)
+    Gx, pGx = _d(Gx)
+    Gy, pGy = _d(Gy)
+    N, KW = E.shape[0], Gx.shape[0]
+    W = N - 2 * erosion
+    ox0, oy0, wx, wy = window if window is not None else (0, 0, W, W)
+    ux = np.empty((wx, wy))
+    uy = np.empty((wx, wy))
+    lib().oracle_conv_window(pE, N, pGx, pGy, KW, erosion, dx * dx, ox0, oy0, wx, wy, ux.ctypes.data_as(_dp),
+                             uy.ctypes.data_as(_dp), nthreads or nthreads_default())
+    return ux, uy
+
+
+def forward(E, I, Gx, Gy, erosion, dx, window=None, nthreads=None, return_u=False):
+    """R = ux*dI/dx + uy*dI/dy on the valid window (srkForwardOaS)."""
+    E, pE = _d(E)
+    I, pI = _d(I)
+    Gx, pGx = _d(Gx)
+    Gy, pGy = _d(Gy)
+    N, KW = E.shape[0], Gx.shape[0]
+    W = N - 2 * erosion
+    ox0, oy0, wx, wy = window if window is not None else (0, 0, W, W)
+    R = np.empty((wx, wy))
+    ux = np.empty((wx, wy))
+    uy = np.empty((wx, wy))
+    lib().oracle_forward_window(pE, pI, N, pGx, pGy, KW, erosion, dx, ox0, oy0, wx, wy, R.ctypes.data_as(_dp),
+                                ux.ctypes.data_as(_dp), uy.ctypes.data_as(_dp), nthreads or nthreads_default())
+    return (R, ux, uy) if return_u else R
+
+
+def adj_wrt_I(v, ux, uy, N, erosion):
+    """dL/dI = Dx^T(ux v) + Dy^T(uy v) on N x N (adjointWrtI)."""
+    wx, pwx = _d(np.asarray(ux) * np.asarray(v))
+    wy, pwy = _d(np.asarray(uy) * np.asarray(v))
+    W = wx.shape[0]
+    out = np.empty((N, N))
+    lib().oracle_adj_wrt_I(pwx, pwy, W, N, erosion, out.ctypes.data_as(_dp))
+    return out
+
+
+def adj_wrt_E(v, I, Gx, Gy, erosion, dx, convention="reference", nthreads=None):
+    """dL/dE on N x N.  convention 'true' = exact adjoint (cpu_adj_wrtE);
+    'reference' = the reference FFT path's convolution with G."""
+    v, pv = _d(v)
+    I, pI = _d(I)
+    Gx, pGx = _d(Gx)
+    Gy, pGy = _d(Gy)
+    N, W, KW = I.shape[0], v.shape[0], Gx.shape[0]
+    out = np.empty((N, N))
+    lib().oracle_adj_wrt_E(pv, pI, pGx, pGy, KW, N, W, erosion, dx, 1 if convention == "reference" else 0,
+                           out.ctypes.data_as(_dp), nthreads or nthreads_default())
+    return out
+
+
+def tangent(f, g, df, dg, Gx, Gy, erosion, dx, nthreads=None):
+    arrs = [_d(a) for a in (f, g, df, dg, Gx, Gy)]
+    N, KW = arrs[0][0].shape[0], arrs[4][0].shape[0]
+    W = N - 2 * erosion
+    dh = np.empty((W, W))
+    lib().oracle_tangent(*[p for _, p in arrs], KW, N, W, erosion, dx, dh.ctypes.data_as(_dp),
+                         nthreads or nthreads_default())
+    return dh
+
+
+def tangent_adjoint(f, g, df, dg, lam, dlam, Gx, Gy, erosion, dx, convention="reference", nthreads=None):
+    arrs = [_d(a) for a in (f, g, df, dg, lam, dlam, Gx, Gy)]
+    N, KW = arrs[0][0].shape[0], arrs[6][0].shape[0]
+    W = N - 2 * erosion
+    dlf = np.empty((N, N))
+    dlg = np.empty((N, N))
+    lib().oracle_tangent_adjoint(*[p for _, p in arrs], KW, N, W, erosion, dx,
+                                 1 if convention == "reference" else 0, dlf.ctypes.data_as(_dp),
+                                 dlg.ctypes.data_as(_dp), nthreads or nthreads_default())
+    return dlf, dlg
+
+
+def make_kernel(kw, dx, gamma, Rw):
+    """(Kx, Ky) float32 (KW, KW) exactly as the reference generates them."""
+    Kx = np.zeros((kw, kw), np.float32)
+    Ky = np.zeros((kw, kw), np.float32)
+    lib().oracle_make_kernel(kw, dx, gamma, Rw, Kx.ctypes.data_as(_fp), Ky.ctypes.data_as(_fp))
+    return Kx, Ky
+
+
+def make_kernel_sigma(kw, sigma_px):
+    """Reference pixel-unit form: gamma = 1/sigma, R_w = 3 sigma, dx = 1
+    (training/main_cd_training.cu:63-77)."""
+    return make_kernel(kw, 1.0, 1.0 / sigma_px, 3.0 * sigma_px)
+
+
+def kernel_freq(K, M):
+    """Reference-layout spectrum (complex64 array of shape (M, M//2+1), [kx, ky])."""
+    K = np.ascontiguousarray(K, np.float32)
+    out = np.empty((M, M // 2 + 1), np.complex64)
+    lib().oracle_kernel_freq(K.ctypes.data_as(_fp), K.shape[0], M, out.view(np.float32).ctypes.data_as(_fp))
+    return out
+
+
+def grf(N, ell, seed):
+    """Seeded Gaussian random field, col-major (N, N) float32: white N(0,1)
+    noise (numpy PCG64, this seed) filtered periodically by exp(-r^2/2 ell^2),
+    then min-max scaled to [0, 1]."""
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((N, N))
+    k = np.fft.fftfreq(N)
+    kk = k[:, None] ** 2 + k[None, :] ** 2
+    H = np.exp(-2.0 * (np.pi ** 2) * (ell ** 2) * kk)
+    x = np.fft.ifft2(np.fft.fft2(w) * H).real
+    x = (x - x.min()) / (x.max() - x.min())
+    return x.astype(np.float32)
+
+
+def ref_host():
+    """The reference's own host generators (None if not built here)."""
+    global _ref_host
+    if _ref_host is None:
+        path = os.path.join(_HERE, "_ref", "libref_host.so")
+        if not os.path.exists(path):
+            return None
+        L = ctypes.CDLL(path)
+        L.ref_gp_field.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _fp]
+        L.ref_lns.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, _fp]
+        _ref_host = L
+    return _ref_host
+
+
+def ref_gp_field(N, ell, seed):
+    """GpGenerator(Covariance2D::isotropic(ell), N, N, seed).generate()."""
+    out = np.empty((N, N), np.float32)
+    ref_host().ref_gp_field(N, ell, seed, out.ctypes.data_as(_fp))
+    return out
+
+
+def ref_lns(vertical, N, sigma_px, period_px=0.0):
+    out = np.empty((N, N), np.float32)
+    ref_host().ref_lns(0 if vertical else 1, N, sigma_px, period_px, out.ctypes.data_as(_fp))
+    return out

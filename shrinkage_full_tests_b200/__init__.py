@@ -1,0 +1,211 @@
+"""B200-native resist-shrinkage operator — Python host mirror of the C ABI.
+
+The operator (pky8903/shrinkage_full_tests)
+
+    h = c * ( conv(Gx, g) * df/dx + conv(Gy, g) * df/dy ),   W = N - 2*erosion
+
+and its derivatives run in hand-written sm_100a kernels inside
+libsrk_b200.so (built in-tree by ``build.py``).  This module loads that
+library through ctypes and exposes the reference's entry points under their
+reference names with the reference's argument order; the workspace argument
+``ws`` is an :class:`SrkPlan`.  Device buffers are torch tensors (or raw
+device addresses given as ``int``); nothing here computes on the host, and
+every entry point raises :class:`SrkError` if the library is missing or a
+call fails.
+"""
+import ctypes
+import os
+
+__all__ = [
+    "SrkError", "SrkPlan", "lib", "srkTrainingForward", "srkForwardOaS", "adjointSRK",
+    "shrinkageTangentOaS", "shrinkageTangentAdjointOaS", "srkPrecomputeKernelFreq", "green_tensor",
+    "forward", "vjp", "jvp", "SRK_ADJ_REFERENCE", "SRK_ADJ_TRUE",
+]
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libsrk_b200.so")
+
+SRK_OK, SRK_ERR_INVALID_ARG, SRK_ERR_UNSUPPORTED, SRK_ERR_ALLOC, SRK_ERR_TIMEOUT, SRK_ERR_CUDA = range(6)
+SRK_F32, SRK_F16, SRK_BF16 = 0, 1, 2
+SRK_ADJ_REFERENCE, SRK_ADJ_TRUE = 0, 1
+
+
+class SrkError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (_STATUS.get(status, status), message))
+        self.status = status
+
+
+_STATUS = {0: "SRK_OK", 1: "SRK_ERR_INVALID_ARG", 2: "SRK_ERR_UNSUPPORTED", 3: "SRK_ERR_ALLOC",
+           4: "SRK_ERR_TIMEOUT", 5: "SRK_ERR_CUDA"}
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("W", ctypes.c_int), ("erosion", ctypes.c_int), ("B_max", ctypes.c_int),
+                ("spectra_M", ctypes.c_int), ("dx", ctypes.c_float), ("tile_M", ctypes.c_int),
+                ("tile_stride", ctypes.c_int), ("tiles", ctypes.c_int), ("tiles_adj", ctypes.c_int),
+                ("chunk_wt", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t), ("dtype", ctypes.c_int)]
+
+
+_lib = None
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_D = ctypes.c_double
+
+# name -> argtypes (restype is srk_status = int unless listed in _RESTYPE)
+_SIGS = {
+    "srk_version": [],
+    "srk_status_string": [_I],
+    "srk_last_error": [],
+    "srk_plan_create": [ctypes.POINTER(_P), _I, _I, _I, _F, _I, _I, _I, _I, ctypes.c_size_t],
+    "srk_plan_destroy": [_P],
+    "srk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
+    "srk_plan_set_adj_convention": [_P, _I],
+    "srk_plan_import_spectra": [_P, _P, _P, _P],
+    "srk_plan_set_kernel": [_P, _P, _P, _I, _P],
+    "srk_green_tensor": [_P, _P, _I, _D, _D, _D, _P],
+    "srk_precompute_kernel_freq": [_P, _I, _I, _P, _P],
+    "srk_training_forward": [_P, _P, _P, _P, _I, _I, _I, _F, _I, _P, _P, _P],
+    "srk_training_forward_sync": [_P, _P, _P, _P, _I, _I, _I, _F, _I, _P, _P, _P],
+    "srk_forward_oas": [_P, _P, _P, _P, _I, _I, _I, _F, _P, _P, _P, _P, _P],
+    "srk_adjoint": [_P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P, _P, _P],
+    "srk_tangent": [_P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P, _P],
+    "srk_tangent_adjoint": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P, _P, _P],
+    "srk_forward": [_P, _P, _I, _P, _P, _P],
+    "srk_vjp": [_P, _P, _P, _I, _P, _P, _P, _P],
+    "srk_jvp": [_P, _P, _P, _P, _I, _P, _P, _P],
+}
+_RESTYPE = {"srk_version": _I, "srk_status_string": ctypes.c_char_p, "srk_last_error": ctypes.c_char_p}
+
+
+def lib():
+    """Load libsrk_b200.so (fails loudly if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise SrkError(SRK_ERR_UNSUPPORTED, "libsrk_b200.so not built at %s (run __graft_entry__.build())"
+                           % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, _I)
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != SRK_OK:
+        raise SrkError(status, lib().srk_last_error().decode())
+
+
+def _ptr(t):
+    """Device address of a torch tensor (or pass-through int / None)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise SrkError(SRK_ERR_INVALID_ARG, "expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise SrkError(SRK_ERR_INVALID_ARG, "expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+class SrkPlan:
+    """Owns the scratch and spectra of one (N, W, erosion, dx) configuration;
+    stands in for the reference's Srk*Workspace structs."""
+
+    def __init__(self, N, W, erosion, dx=1.0, B_max=1, spectra_M=None, dtype=SRK_F32, tile_M=0,
+                 scratch_budget=0):
+        h = _P()
+        _check(lib().srk_plan_create(ctypes.byref(h), N, W, erosion, dx, B_max,
+                                     spectra_M if spectra_M is not None else N, dtype, tile_M, scratch_budget))
+        self.handle = h.value
+        self.N, self.W, self.erosion, self.dx, self.B_max = N, W, erosion, dx, B_max
+
+    def info(self):
+        i = PlanInfo()
+        _check(lib().srk_plan_get_info(self.handle, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in PlanInfo._fields_}
+
+    def set_adj_convention(self, conv):
+        _check(lib().srk_plan_set_adj_convention(self.handle, conv))
+
+    def import_spectra(self, Gx_freq, Gy_freq, stream=None):
+        _check(lib().srk_plan_import_spectra(self.handle, _ptr(Gx_freq), _ptr(Gy_freq), _stream(stream)))
+
+    def set_kernel(self, Kx, Ky, stream=None):
+        _check(lib().srk_plan_set_kernel(self.handle, _ptr(Kx), _ptr(Ky), Kx.shape[-1], _stream(stream)))
+
+    def destroy(self):
+        if self.handle:
+            lib().srk_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def srkTrainingForward(E, I, Gx_freq, Gy_freq, N, W, erosion, dx, B, stream, R, ws):
+    _check(lib().srk_training_forward(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, B,
+                                      _stream(stream), _ptr(R), ws.handle))
+
+
+def srkForwardOaS(E, I, Gx_freq, Gy_freq, N, W, erosion, dx, stream, R, ws, ux=None, uy=None):
+    _check(lib().srk_forward_oas(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx,
+                                 _stream(stream), _ptr(R), ws.handle, _ptr(ux), _ptr(uy)))
+
+
+def adjointSRK(v, ux, uy, I, Gx_freq, Gy_freq, N, W, erosion, dx, stream, dLdI, dLdE, ws):
+    _check(lib().srk_adjoint(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion,
+                             dx, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
+
+
+def shrinkageTangentOaS(f, g, df, dg, Gx_freq, Gy_freq, N, W, erosion, dx, stream, dh, ws):
+    _check(lib().srk_tangent(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion,
+                             dx, _stream(stream), _ptr(dh), ws.handle))
+
+
+def shrinkageTangentAdjointOaS(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_freq, N, W, erosion, dx, stream,
+                               dLam_f, dLam_g, ws):
+    _check(lib().srk_tangent_adjoint(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
+                                     _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, _stream(stream),
+                                     _ptr(dLam_f), _ptr(dLam_g), ws.handle))
+
+
+def srkPrecomputeKernelFreq(K, kw, kh, M, G_freq, stream=None):
+    """Spectrum of a (kw x kh, kw == kh) device kernel at size M, reference layout."""
+    if kw != kh:
+        raise SrkError(SRK_ERR_UNSUPPORTED, "square kernels only")
+    _check(lib().srk_precompute_kernel_freq(_ptr(K), kw, M, _ptr(G_freq), _stream(stream)))
+
+
+def green_tensor(Kx, Ky, gamma, R_w, dx, stream=None):
+    """Fill device tensors Kx, Ky (KW x KW) with the FP64-evaluated Green's tensor."""
+    _check(lib().srk_green_tensor(_ptr(Kx), _ptr(Ky), Kx.shape[-1], gamma, R_w, dx, _stream(stream)))
+
+
+def forward(f, g, B, h, ws, stream=None):
+    _check(lib().srk_forward(_ptr(f), _ptr(g), B, _stream(stream), _ptr(h), ws.handle))
+
+
+def vjp(v, f, g, B, dLdf, dLdg, ws, stream=None):
+    _check(lib().srk_vjp(_ptr(v), _ptr(f), _ptr(g), B, _stream(stream), _ptr(dLdf), _ptr(dLdg), ws.handle))
+
+
+def jvp(f, g, df, dg, B, dh, ws, stream=None):
+    _check(lib().srk_jvp(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), B, _stream(stream), _ptr(dh), ws.handle))

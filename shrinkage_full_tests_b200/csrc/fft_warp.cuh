@@ -1,0 +1,165 @@
+// fft_warp.cuh — one-warp complex FFT of length M (128..1024) for sm_100a.
+//
+// Layout contract (both directions):
+//   lane t holds x[i] = X[t + 32*i], i in [0, M/32)      ("strided" order)
+// so a warp loads/stores one contiguous column of M complex values with
+// fully coalesced 256-byte requests, and the transform result comes back in
+// the same order (natural frequency order, no bit reversal).
+//
+// Algorithm: Stockham auto-sort, one radix-R pass per stage (mixed radix,
+// R in {2,4,8,16}).  Pass p with span Ns (product of the previous radices)
+// runs M/R butterflies; butterfly j reads x[j + r*M/R], multiplies by
+// W_{Ns*R}^{r*(j mod Ns)}, does an R-point DFT and writes
+// y[(j/Ns)*Ns*R + (j mod Ns) + r*Ns].  Each lane owns EPT/R butterflies
+// (j = t + 32*b), so the first pass reads straight from registers and the
+// last pass writes straight back to registers in strided order; the
+// passes in between exchange through a per-warp shared-memory row of
+// M + M/16 float2 (one pad word per 16, which makes the scatter of the
+// first pass bank-conflict free).
+//
+// Twiddles W_M^m = exp(-2*pi*i*m/M) come from a table in shared memory that
+// the host fills from double-precision cos/sin (rounded once to float);
+// the inverse transform uses their conjugates.  The transforms are
+// unnormalised in both directions.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace srk {
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <bool INV>
+__device__ __forceinline__ float2 twmul(float2 a, float2 w) {
+  return INV ? cmulc(a, w) : cmul(a, w);
+}
+
+__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int fft_row_words(int M) { return M + M / 16; }
+
+// Multiply by W_16^m = exp(-+ i*pi*m/8) for a compile-time m in [0,8).
+template <int m, bool INV>
+__device__ __forceinline__ float2 rot16(float2 v) {
+  constexpr float R2 = 0.70710678118654752440f;   // cos(pi/4)
+  constexpr float C1 = 0.92387953251128675613f;   // cos(pi/8)
+  constexpr float S1 = 0.38268343236508977173f;   // sin(pi/8)
+  if constexpr (m == 0) {
+    return v;
+  } else if constexpr (m == 4) {                  // -i (forward) / +i (inverse)
+    return INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+  } else if constexpr (m == 2) {                  // (1 -+ i)/sqrt2
+    return INV ? make_float2((v.x - v.y) * R2, (v.x + v.y) * R2)
+               : make_float2((v.x + v.y) * R2, (v.y - v.x) * R2);
+  } else if constexpr (m == 6) {                  // (-1 -+ i)/sqrt2
+    return INV ? make_float2(-(v.x + v.y) * R2, (v.x - v.y) * R2)
+               : make_float2((v.y - v.x) * R2, -(v.x + v.y) * R2);
+  } else {
+    constexpr float c = (m == 1) ? C1 : (m == 3) ? S1 : (m == 5) ? -S1 : -C1;
+    constexpr float s = (m == 1) ? S1 : (m == 3) ? C1 : (m == 5) ? C1 : S1;
+    // forward: v*(c - i s); inverse: v*(c + i s)
+    return INV ? make_float2(v.x * c - v.y * s, v.y * c + v.x * s)
+               : make_float2(v.x * c + v.y * s, v.y * c - v.x * s);
+  }
+}
+
+// In-register R-point DFT (natural order in and out), radix-2 decimation in
+// time applied recursively.
+template <int R, bool INV>
+struct Dft {
+  template <int K>
+  __device__ __forceinline__ static void combine(float2* a, const float2* e, const float2* o) {
+    if constexpr (K < R / 2) {
+      const float2 t = rot16<(16 / R) * K, INV>(o[K]);
+      a[K] = cadd(e[K], t);
+      a[K + R / 2] = csub(e[K], t);
+      combine<K + 1>(a, e, o);
+    }
+  }
+  __device__ __forceinline__ static void run(float2* a) {
+    float2 e[R / 2], o[R / 2];
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) { e[i] = a[2 * i]; o[i] = a[2 * i + 1]; }
+    Dft<R / 2, INV>::run(e);
+    Dft<R / 2, INV>::run(o);
+    combine<0>(a, e, o);
+  }
+};
+template <bool INV>
+struct Dft<2, INV> {
+  __device__ __forceinline__ static void run(float2* a) {
+    const float2 t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+  }
+};
+
+// One Stockham pass.  sm: this warp's padded exchange row; tw: W_M table.
+template <int M, int R, int NS, bool FIRST, bool LAST, bool INV>
+__device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict__ sm,
+                                         const float2* __restrict__ tw, int lane) {
+  constexpr int EPT = M / 32;
+  constexpr int NB = EPT / R;
+  static_assert(EPT % R == 0, "radix must divide elements per lane");
+  if constexpr (!FIRST) {
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) x[i] = sm[fft_pad(lane + 32 * i)];
+    __syncwarp();
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    float2 a[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = x[b + r * NB];
+    const int j = lane + 32 * b;
+    const int k = j & (NS - 1);
+    if constexpr (!FIRST) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], tw[r * k * (M / (NS * R))]);
+    }
+    Dft<R, INV>::run(a);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[b + r * NB] = a[r];
+    } else {
+      const int base = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[fft_pad(base + r * NS)] = a[r];
+    }
+  }
+  if constexpr (!LAST) __syncwarp();
+}
+
+// Full transform.  All 32 lanes of the warp must call it together.
+template <int M, bool INV>
+__device__ __forceinline__ void fft(float2 (&x)[M / 32], float2* __restrict__ sm,
+                                    const float2* __restrict__ tw, int lane) {
+  __syncwarp();  // the row may still be read by lanes finishing a previous use
+  if constexpr (M == 128) {
+    fft_pass<M, 4, 1, true, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 4, 4, false, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 4, 16, false, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 2, 64, false, true, INV>(x, sm, tw, lane);
+  } else if constexpr (M == 256) {
+    fft_pass<M, 8, 1, true, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 8, 8, false, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 4, 64, false, true, INV>(x, sm, tw, lane);
+  } else if constexpr (M == 512) {
+    fft_pass<M, 8, 1, true, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 8, 8, false, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 8, 64, false, true, INV>(x, sm, tw, lane);
+  } else if constexpr (M == 1024) {
+    fft_pass<M, 16, 1, true, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 8, 16, false, false, INV>(x, sm, tw, lane);
+    fft_pass<M, 8, 128, false, true, INV>(x, sm, tw, lane);
+  } else {
+    static_assert(M == 128 || M == 256 || M == 512 || M == 1024, "unsupported FFT length");
+  }
+}
+
+}  // namespace srk
