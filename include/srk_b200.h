@@ -51,6 +51,14 @@ typedef enum srk_dtype { SRK_F32 = 0, SRK_F16 = 1, SRK_BF16 = 2 } srk_dtype;
  * for even kernels and differ by a sign for the odd Green's tensor. */
 typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_adj_convention;
 
+/* Kernel schedule of the convolution engine.  PERSISTENT (default): one
+ * launch per call; the column/row/column passes of every work tile run as
+ * tickets of a queue with their intermediates in an L2-resident ring.
+ * THREE_PASS: three launches per chunk of work tiles with the intermediates
+ * in a device scratch buffer (used for A/B measurement and as the fallback
+ * when the scratch budget holds fewer than three work tiles). */
+typedef enum srk_schedule { SRK_SCHEDULE_PERSISTENT = 0, SRK_SCHEDULE_THREE_PASS = 1 } srk_schedule;
+
 typedef struct srk_plan_info {
   int N, W, erosion, B_max, spectra_M;
   float dx;
@@ -61,6 +69,9 @@ typedef struct srk_plan_info {
   int chunk_wt;     /* work tiles per scratch chunk */
   size_t scratch_bytes;
   srk_dtype dtype;
+  int schedule;       /* srk_schedule */
+  int last_launches;  /* kernel launches of the last engine call */
+  int last_grid;      /* CTAs of the last persistent launch */
 } srk_plan_info;
 
 /* ---- library ------------------------------------------------------------ */
@@ -82,6 +93,15 @@ srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, 
 srk_status srk_plan_destroy(srk_plan plan);
 srk_status srk_plan_get_info(srk_plan plan, srk_plan_info* info);
 srk_status srk_plan_set_adj_convention(srk_plan plan, srk_adj_convention conv);
+srk_status srk_plan_set_schedule(srk_plan plan, srk_schedule schedule);
+/* Synchronise `stream` and report a device-side failure of the plan's last
+ * persistent launch (SRK_ERR_TIMEOUT if a bounded wait gave up).  Operators
+ * also report such a failure of the previous call once it has completed. */
+srk_status srk_plan_sync(srk_plan plan, srk_stream_t stream);
+/* Failure-path self test: one CTA waits, bounded by spin_limit polls, for a
+ * counter that nothing increments.  Returns SRK_ERR_TIMEOUT when the wait
+ * gave up as designed (the context stays usable), SRK_OK never. */
+srk_status srk_debug_wait_selftest(srk_plan plan, unsigned long long spin_limit, srk_stream_t stream);
 
 /* Import caller spectra (reference layout, size spectra_M).  Done implicitly
  * by the operators whenever they see spectrum pointers different from the

@@ -28,6 +28,7 @@ LIB_PATH = os.path.join(_PKG, "libsrk_b200.so")
 SRK_OK, SRK_ERR_INVALID_ARG, SRK_ERR_UNSUPPORTED, SRK_ERR_ALLOC, SRK_ERR_TIMEOUT, SRK_ERR_CUDA = range(6)
 SRK_F32, SRK_F16, SRK_BF16 = 0, 1, 2
 SRK_ADJ_REFERENCE, SRK_ADJ_TRUE = 0, 1
+SRK_SCHEDULE_PERSISTENT, SRK_SCHEDULE_THREE_PASS = 0, 1
 
 
 class SrkError(RuntimeError):
@@ -44,7 +45,8 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("W", ctypes.c_int), ("erosion", ctypes.c_int), ("B_max", ctypes.c_int),
                 ("spectra_M", ctypes.c_int), ("dx", ctypes.c_float), ("tile_M", ctypes.c_int),
                 ("tile_stride", ctypes.c_int), ("tiles", ctypes.c_int), ("tiles_adj", ctypes.c_int),
-                ("chunk_wt", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t), ("dtype", ctypes.c_int)]
+                ("chunk_wt", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t), ("dtype", ctypes.c_int),
+                ("schedule", ctypes.c_int), ("last_launches", ctypes.c_int), ("last_grid", ctypes.c_int)]
 
 
 _lib = None
@@ -62,6 +64,9 @@ _SIGS = {
     "srk_plan_destroy": [_P],
     "srk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "srk_plan_set_adj_convention": [_P, _I],
+    "srk_plan_set_schedule": [_P, _I],
+    "srk_plan_sync": [_P, _P],
+    "srk_debug_wait_selftest": [_P, ctypes.c_ulonglong, _P],
     "srk_plan_import_spectra": [_P, _P, _P, _P],
     "srk_plan_set_kernel": [_P, _P, _P, _I, _P],
     "srk_green_tensor": [_P, _P, _I, _D, _D, _D, _P],
@@ -141,6 +146,18 @@ class SrkPlan:
 
     def set_adj_convention(self, conv):
         _check(lib().srk_plan_set_adj_convention(self.handle, conv))
+
+    def set_schedule(self, schedule):
+        _check(lib().srk_plan_set_schedule(self.handle, schedule))
+
+    def sync(self, stream=None):
+        """Synchronise and raise SrkError(SRK_ERR_TIMEOUT) if a bounded
+        device-side wait of the last launch gave up."""
+        _check(lib().srk_plan_sync(self.handle, _stream(stream)))
+
+    def wait_selftest(self, spin_limit=1 << 12, stream=None):
+        """Return the status of the bounded-wait self test (SRK_ERR_TIMEOUT expected)."""
+        return lib().srk_debug_wait_selftest(self.handle, spin_limit, _stream(stream))
 
     def import_spectra(self, Gx_freq, Gy_freq, stream=None):
         _check(lib().srk_plan_import_spectra(self.handle, _ptr(Gx_freq), _ptr(Gy_freq), _stream(stream)))

@@ -269,13 +269,19 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
   }
 }
 
-// ---- kernels ---------------------------------------------------------------
+// ---- phases ------------------------------------------------------------------
 constexpr int kWarps = 8;
 constexpr int kThreads = 32 * kWarps;
 
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int M) {
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
 }
+
+// Scratch of one work tile: S1 [K][M][M] then S2 [L][S][M] (float2).
+template <int M, int OP>
+__host__ __device__ constexpr size_t s1_elems() { return (size_t)OpTraits<OP>::K * M * M; }
+template <int M, int OP>
+__host__ __device__ inline size_t wt_elems(int S) { return s1_elems<M, OP>() + (size_t)OpTraits<OP>::L * S * M; }
 
 template <int M>
 constexpr size_t p1_smem_bytes() { return sizeof(float2) * (M + kWarps * fft_row_words(M)); }
@@ -285,65 +291,57 @@ inline size_t p2_smem_bytes(int M, int K, int L, int S) {
   return sizeof(float2) * ((size_t)M + (size_t)K * kWarps * fft_row_words(M) + (size_t)L * S * 9);
 }
 
-// P1: grid (M/8, K, WTs in chunk).  One warp per column.
+// P1: warp `warp` transforms column x = xb*8 + warp of every field along y.
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, 2)
-k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ S1) {
+__device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
+                                       float2* __restrict__ row, const float2* __restrict__ tw, int warp, int lane) {
   constexpr int EPT = M / 32;
   constexpr int K = OpTraits<OP>::K;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* row = sm + M + warp * fft_row_words(M);
-  load_twiddles(tw, twg, M);
-  __syncthreads();
-  const int x = blockIdx.x * kWarps + warp;
-  const int k = blockIdx.y;
-  const int wl = blockIdx.z;
-  float2 z[EPT];
-  load_column<M, OP, T>(a, g, w0 + wl, k, x, lane, z);
-  fft<M, false>(z, row, tw, lane);
-  float2* dst = S1 + ((size_t)(wl * K + k) * M + x) * M;
+  const int x = xb * kWarps + warp;
+#pragma unroll 1
+  for (int k = 0; k < K; ++k) {
+    float2 z[EPT];
+    load_column<M, OP, T>(a, g, w, k, x, lane, z);
+    fft<M, false>(z, row, tw, lane);
+    float2* dst = S1 + ((size_t)k * M + x) * M + lane;
 #pragma unroll
-  for (int i = 0; i < EPT; ++i) dst[lane + 32 * i] = z[i];
+    for (int i = 0; i < EPT; ++i) __stcg(dst + 32 * i, z[i]);
+  }
 }
 
-// P2: grid (M/8, WTs in chunk).  One warp per row ky.
+// P2: rows ky0 .. ky0+7: FFT along x, spectral map, inverse, keep the valid
+// columns, write S2 column-contiguous through a padded transpose buffer.
+// Needs __syncthreads-uniform control flow (all threads of the CTA).
 template <int M, int OP>
-__global__ void __launch_bounds__(kThreads, 2)
-k_p2(const float2* __restrict__ S1, float2* __restrict__ S2, const float2* __restrict__ Gx,
-     const float2* __restrict__ Gy, int conjG, Geom g, const float2* __restrict__ twg) {
+__device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __restrict__ S2,
+                                       const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
+                                       const Geom& g, int ky0, float2* __restrict__ buf,
+                                       const float2* __restrict__ tw, int warp, int lane) {
   constexpr int EPT = M / 32;
   constexpr int K = OpTraits<OP>::K;
   constexpr int L = OpTraits<OP>::L;
   constexpr int RW = fft_row_words(M);
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  float2* in = sm + M;                   // [K][8][RW]
-  float2* out = in + K * kWarps * RW;    // [L][S][9]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wl = blockIdx.y;
-  const int ky0 = blockIdx.x * kWarps;
+  float2* in = buf;                      // [K][8][RW]
+  float2* out = buf + K * kWarps * RW;   // [L][S][9]
   const int S = g.S, e = g.e;
-  load_twiddles(tw, twg, M);
   for (int idx = threadIdx.x; idx < K * M * 4; idx += kThreads) {
     const int k = idx / (M * 4);
     const int rem = idx - k * (M * 4);
     const int x = rem >> 2, rp = rem & 3;
-    const float4 q = __ldcs(reinterpret_cast<const float4*>(S1 + ((size_t)(wl * K + k) * M + x) * M + ky0 + 2 * rp));
+    const float4 q = __ldcg(reinterpret_cast<const float4*>(S1 + ((size_t)k * M + x) * M + ky0 + 2 * rp));
     in[(k * kWarps + 2 * rp) * RW + fft_pad(x)] = make_float2(q.x, q.y);
     in[(k * kWarps + 2 * rp + 1) * RW + fft_pad(x)] = make_float2(q.z, q.w);
   }
   __syncthreads();
-
   const int ky = ky0 + warp;
   float2* row0 = in + warp * RW;
+  const float2* rd0 = row0 + lane + (lane >> 4);
   float2 z0[EPT];
 #pragma unroll
-  for (int i = 0; i < EPT; ++i) z0[i] = row0[fft_pad(lane + 32 * i)];
+  for (int i = 0; i < EPT; ++i) z0[i] = rd0[34 * i];
   fft<M, false>(z0, row0, tw, lane);
-  const float2* gxr = Gx + (size_t)ky * M;
-  const float2* gyr = Gy + (size_t)ky * M;
+  const float2* gxr = Gx + (size_t)ky * M + lane;
+  const float2* gyr = Gy + (size_t)ky * M + lane;
   auto spec = [&](float2 z, float2 G) { return conjG ? cmulc(z, G) : cmul(z, G); };
   auto park = [&](const float2 (&o)[EPT], int l) {
 #pragma unroll
@@ -355,22 +353,22 @@ k_p2(const float2* __restrict__ S1, float2* __restrict__ S2, const float2* __res
   if constexpr (K == 1) {
     float2 o[EPT];
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gxr + lane + 32 * i));
+    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gxr + 32 * i));
     fft<M, true>(o, row0, tw, lane);
     park(o, 0);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gyr + lane + 32 * i));
+    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gyr + 32 * i));
     fft<M, true>(o, row0, tw, lane);
     park(o, 1);
   } else {
     float2* row1 = in + (kWarps + warp) * RW;
+    const float2* rd1 = row1 + lane + (lane >> 4);
     float2 z1[EPT];
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) z1[i] = row1[fft_pad(lane + 32 * i)];
+    for (int i = 0; i < EPT; ++i) z1[i] = rd1[34 * i];
     fft<M, false>(z1, row1, tw, lane);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i)
-      z0[i] = cadd(spec(z0[i], __ldg(gxr + lane + 32 * i)), spec(z1[i], __ldg(gyr + lane + 32 * i)));
+    for (int i = 0; i < EPT; ++i) z0[i] = cadd(spec(z0[i], __ldg(gxr + 32 * i)), spec(z1[i], __ldg(gyr + 32 * i)));
     fft<M, true>(z0, row0, tw, lane);
     park(z0, 0);
   }
@@ -381,43 +379,190 @@ k_p2(const float2* __restrict__ S1, float2* __restrict__ S2, const float2* __res
     const int xv = rem >> 2, rp = rem & 3;
     const float2 lo = out[(l * S + xv) * 9 + 2 * rp];
     const float2 hi = out[(l * S + xv) * 9 + 2 * rp + 1];
-    __stcs(reinterpret_cast<float4*>(S2 + ((size_t)(wl * L + l) * S + xv) * M + ky0 + 2 * rp),
+    __stcg(reinterpret_cast<float4*>(S2 + ((size_t)l * S + xv) * M + ky0 + 2 * rp),
            make_float4(lo.x, lo.y, hi.x, hi.y));
   }
 }
 
-// P3: grid (ceil(S/8), WTs in chunk).  One warp per valid column.
+// P3: warp `warp` finishes valid column xv = xb*8 + warp (if < S).
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, 2)
-k_p3(const float2* __restrict__ S2, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
+__device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
+                                       float2* __restrict__ row, const float2* __restrict__ tw, int warp, int lane) {
   constexpr int EPT = M / 32;
   constexpr int L = OpTraits<OP>::L;
-  extern __shared__ float2 sm[];
-  float2* tw = sm;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float2* row = sm + M + warp * fft_row_words(M);
-  load_twiddles(tw, twg, M);
-  __syncthreads();
-  const int xv = blockIdx.x * kWarps + warp;
+  const int xv = xb * kWarps + warp;
   if (xv >= g.S) return;
-  const int wl = blockIdx.y;
   float2 z0[EPT], z1[EPT];
   {
-    const float2* src = S2 + ((size_t)(wl * L + 0) * g.S + xv) * M;
+    const float2* src = S2 + (size_t)xv * M + lane;
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) z0[i] = __ldcs(src + lane + 32 * i);
+    for (int i = 0; i < EPT; ++i) z0[i] = __ldcg(src + 32 * i);
     fft<M, true>(z0, row, tw, lane);
   }
   if constexpr (L == 2) {
-    const float2* src = S2 + ((size_t)(wl * L + 1) * g.S + xv) * M;
+    const float2* src = S2 + ((size_t)g.S + xv) * M + lane;
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) z1[i] = __ldcs(src + lane + 32 * i);
+    for (int i = 0; i < EPT; ++i) z1[i] = __ldcg(src + 32 * i);
     fft<M, true>(z1, row, tw, lane);
   } else {
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z1[i] = make_float2(0.f, 0.f);
   }
-  epilogue_column<M, OP, T>(a, g, w0 + wl, xv + g.e, lane, z0, z1);
+  epilogue_column<M, OP, T>(a, g, w, xv + g.e, lane, z0, z1);
+}
+
+// ---- three-launch schedule (one kernel per phase over a chunk of WTs) ------
+template <int M, int OP, typename T>
+__global__ void __launch_bounds__(kThreads, 2)
+k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
+  extern __shared__ float2 sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  load_twiddles(sm, twg, M);
+  __syncthreads();
+  const int wl = blockIdx.y;
+  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + warp * fft_row_words(M),
+                   sm, warp, lane);
+}
+
+template <int M, int OP>
+__global__ void __launch_bounds__(kThreads, 2)
+k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG, Geom g,
+     const float2* __restrict__ twg) {
+  extern __shared__ float2 sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  load_twiddles(sm, twg, M);
+  float2* base = scratch + blockIdx.y * wt_elems<M, OP>(g.S);
+  phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, blockIdx.x * kWarps, sm + M, sm, warp, lane);
+}
+
+template <int M, int OP, typename T>
+__global__ void __launch_bounds__(kThreads, 2)
+k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
+  extern __shared__ float2 sm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  load_twiddles(sm, twg, M);
+  __syncthreads();
+  const int wl = blockIdx.y;
+  phase3<M, OP, T>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
+                   sm + M + warp * fft_row_words(M), sm, warp, lane);
+}
+
+// ---- persistent schedule ---------------------------------------------------------
+// One launch processes every WT.  Work is a ticket queue of rounds; round r
+// holds the P1 units of WT r, the P2 units of WT r-kLag and the P3 units of
+// WT r-2*kLag.  A WT's scratch lives in slot w mod nslot of a small ring that
+// stays in L2.  Per-slot counters (monotonic over the slot's reuses) order
+// the phases:
+//   P1(w) needs c2[slot] >= gen*n2       (previous user's P2 done reading S1)
+//   P2(w) needs c1[slot] >= (gen+1)*n1   (its S1 complete)
+//           and c3[slot] >= gen*n3       (previous user's P3 done reading S2)
+//   P3(w) needs c2[slot] >= (gen+1)*n2   (its S2 complete)
+// Every dependency points to a smaller ticket, and a ticket is only ever held
+// by a running CTA, so the smallest unfinished ticket can always proceed.
+// Waits are bounded anyway: a wait that exceeds `spin_limit` polls sets
+// ctl->abort (with the place in ctl->where) and every CTA returns.
+constexpr int kLag = 2;
+constexpr int kMaxSlots = 16;
+
+struct Ctl {
+  unsigned int ticket;
+  unsigned int abort;
+  unsigned int where;
+  unsigned int pad;
+  unsigned int c1[kMaxSlots], c2[kMaxSlots], c3[kMaxSlots];
+};
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Thread-0 wait: returns false if the kernel must stop.
+__device__ __forceinline__ bool wait_geq(const unsigned int* p, unsigned int target, unsigned long long limit,
+                                         Ctl* ctl, unsigned int where) {
+  unsigned long long it = 0;
+  while (ld_acquire(p) < target) {
+    if (ld_acquire(&ctl->abort)) return false;
+    if (++it > limit) {
+      atomicExch(&ctl->where, where);
+      atomicExch(&ctl->abort, 1u);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  return true;
+}
+
+template <int M, int OP, typename T>
+__global__ void __launch_bounds__(kThreads, 2)
+k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
+          const float2* __restrict__ twg, float2* __restrict__ scratch, int nslot, int nwt, Ctl* ctl,
+          unsigned long long spin_limit) {
+  extern __shared__ float2 sm[];
+  __shared__ int s_t[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n1 = M / kWarps, n2 = M / kWarps, n3 = (g.S + kWarps - 1) / kWarps;
+  const int round = n1 + n2 + n3;
+  const long long total = (long long)(nwt + 2 * kLag) * round;
+  const size_t slot_elems = wt_elems<M, OP>(g.S);
+  float2* tw = sm;
+  float2* buf = sm + M;
+  load_twiddles(tw, twg, M);
+  if (threadIdx.x == 0) s_t[0] = (int)atomicAdd(&ctl->ticket, 1u);
+  __syncthreads();
+  int cur = s_t[0];
+  while (cur < total) {
+    // prefetch the next ticket while this unit runs
+    unsigned int nxt = 0;
+    if (threadIdx.x == 0) nxt = atomicAdd(&ctl->ticket, 1u);
+    const int r = cur / round, u = cur - (cur / round) * round;
+    int phase, w, unit;
+    if (u < n1) { phase = 1; w = r; unit = u; }
+    else if (u < n1 + n2) { phase = 2; w = r - kLag; unit = u - n1; }
+    else { phase = 3; w = r - 2 * kLag; unit = u - n1 - n2; }
+    const bool live = (w >= 0 && w < nwt);
+    const int slot = live ? w % nslot : 0;
+    const unsigned int gen = live ? (unsigned int)(w / nslot) : 0u;
+    if (threadIdx.x == 0) {
+      bool ok = ld_acquire(&ctl->abort) == 0u;
+      if (ok && live) {
+        if (phase == 1) ok = wait_geq(&ctl->c2[slot], gen * n2, spin_limit, ctl, 1);
+        else if (phase == 2) ok = wait_geq(&ctl->c1[slot], (gen + 1) * n1, spin_limit, ctl, 2) &&
+                                  wait_geq(&ctl->c3[slot], gen * n3, spin_limit, ctl, 3);
+        else ok = wait_geq(&ctl->c2[slot], (gen + 1) * n2, spin_limit, ctl, 4);
+      }
+      s_t[1] = ok ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_t[1]) return;
+    if (live) {
+      float2* base = scratch + (size_t)slot * slot_elems;
+      if (phase == 1) {
+        phase1<M, OP, T>(a, g, w, unit, base, buf + warp * fft_row_words(M), tw, warp, lane);
+      } else if (phase == 2) {
+        phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * kWarps, buf, tw, warp, lane);
+      } else {
+        phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf + warp * fft_row_words(M), tw, warp, lane);
+      }
+    }
+    __syncthreads();  // every thread's scratch stores of this unit are issued
+    if (threadIdx.x == 0) {
+      if (live) {
+        __threadfence();
+        atomicAdd(phase == 1 ? &ctl->c1[slot] : phase == 2 ? &ctl->c2[slot] : &ctl->c3[slot], 1u);
+      }
+      s_t[0] = (int)nxt;
+    }
+    __syncthreads();
+    cur = s_t[0];
+  }
+}
+
+// Bounded-wait self test: thread 0 of one CTA waits for a counter that
+// nothing increments; the wait must give up and raise the abort flag.
+__global__ void k_wait_selftest(Ctl* ctl, unsigned long long spin_limit) {
+  if (threadIdx.x == 0) wait_geq(&ctl->c1[0], 1u, spin_limit, ctl, 99);
 }
 
 // dL/df = D_x^T(wx) + D_y^T(wy) on N x N, with wx, wy given on the W x W

@@ -99,6 +99,29 @@ struct Dft<2, INV> {
   }
 };
 
+// Per-lane part P(lane) and compile-time part C(b, r) of the write index
+// (j/NS)*NS*R + (j mod NS) + r*NS of butterfly j = lane + 32*b.
+template <int R, int NS>
+__host__ __device__ constexpr int pass_P(int lane) {
+  return NS >= 32 ? lane : (lane / NS) * NS * R + (lane % NS);
+}
+template <int R, int NS>
+__host__ __device__ constexpr int pass_C(int b, int r) {
+  return NS >= 32 ? ((32 * b) / NS) * NS * R + (32 * b) % NS + r * NS : 32 * b * R + r * NS;
+}
+// fft_pad(P + C) == fft_pad(P) + fft_pad(C) for every lane, butterfly and
+// leg: then every shared-memory write is (per-lane base) + (immediate).
+template <int M, int R, int NS>
+__host__ __device__ constexpr bool pad_separable() {
+  for (int lane = 0; lane < 32; ++lane)
+    for (int b = 0; b < M / 32 / R; ++b)
+      for (int r = 0; r < R; ++r) {
+        const int P = pass_P<R, NS>(lane), C = pass_C<R, NS>(b, r);
+        if (fft_pad(P + C) != fft_pad(P) + fft_pad(C)) return false;
+      }
+  return true;
+}
+
 // One Stockham pass.  sm: this warp's padded exchange row; tw: W_M table.
 template <int M, int R, int NS, bool FIRST, bool LAST, bool INV>
 __device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict__ sm,
@@ -106,30 +129,36 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict
   constexpr int EPT = M / 32;
   constexpr int NB = EPT / R;
   static_assert(EPT % R == 0, "radix must divide elements per lane");
+  static_assert(LAST || pad_separable<M, R, NS>(), "padded write index must split into base + immediate");
   if constexpr (!FIRST) {
+    // fft_pad(lane + 32 i) = lane + (lane >> 4) + 34 i
+    const float2* rd = sm + lane + (lane >> 4);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) x[i] = sm[fft_pad(lane + 32 * i)];
+    for (int i = 0; i < EPT; ++i) x[i] = rd[34 * i];
     __syncwarp();
   }
+  float2* wr = nullptr;
+  if constexpr (!LAST) wr = sm + fft_pad(pass_P<R, NS>(lane));
+  // twiddle exponent step: W_{NS*R}^{r k} = W_M^{r k (M/(NS R))}
+  constexpr int TS = M / (NS * R);
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     float2 a[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) a[r] = x[b + r * NB];
-    const int j = lane + 32 * b;
-    const int k = j & (NS - 1);
     if constexpr (!FIRST) {
+      // k = (lane + 32 b) mod NS
+      const int k = (NS <= 32) ? (lane & (NS - 1)) : (lane + ((32 * b) & (NS - 1)));
 #pragma unroll
-      for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], tw[r * k * (M / (NS * R))]);
+      for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], tw[r * k * TS]);
     }
     Dft<R, INV>::run(a);
     if constexpr (LAST) {
 #pragma unroll
       for (int r = 0; r < R; ++r) x[b + r * NB] = a[r];
     } else {
-      const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[fft_pad(base + r * NS)] = a[r];
+      for (int r = 0; r < R; ++r) wr[fft_pad(pass_C<R, NS>(b, r))] = a[r];
     }
   }
   if constexpr (!LAST) __syncwarp();

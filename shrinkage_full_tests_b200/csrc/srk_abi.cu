@@ -74,13 +74,20 @@ struct srk_plan_s {
   size_t scratch_bytes = 0;
   float* wbuf = nullptr;               // wx, wy for dL/df
   size_t wbuf_bytes = 0;
+  int schedule = SRK_SCHEDULE_PERSISTENT;
+  Ctl* ctl = nullptr;                  // persistent-kernel control block
+  unsigned int* mailbox = nullptr;     // pinned host copy of (abort, where)
+  cudaEvent_t mailbox_ev = nullptr;
+  bool mailbox_pending = false;
+  unsigned long long spin_limit = 1ull << 24;
+  int last_grid = 0, last_launches = 0;
 };
 
 namespace {
 
 // ---- tile choice -------------------------------------------------------------
-// FFT work per image ~ T^2 * M^2 * log2(M); choose the cheapest M whose
-// valid stride S = M - 2e keeps at least 16 outputs.
+// FFT work per image ~ T^2 * M^2 * log2(M) for the forward geometry; choose
+// the cheapest M whose valid stride S = M - 2e keeps at least 16 outputs.
 int choose_tile(int N, int W, int e) {
   const int cand[3] = {128, 256, 512};
   int best = 0;
@@ -89,9 +96,8 @@ int choose_tile(int N, int W, int e) {
     const int S = M - 2 * e;
     if (S < 16) continue;
     const int T = (W + S - 1) / S;
-    const int Ta = (N + S - 1) / S;
     const double lg = std::log2((double)M);
-    const double cost = (double)T * T * M * M * lg + 0.5 * (double)Ta * Ta * M * M * lg;
+    const double cost = (double)T * T * M * M * lg;
     if (best == 0 || cost < best_cost * 0.98) { best = M; best_cost = cost; }
   }
   return best;
@@ -131,18 +137,42 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   const size_t sm1 = p1_smem_bytes<M>();
   const size_t sm2 = p2_smem_bytes(M, K, L, g.S);
   const size_t sm3 = p3_smem_bytes<M>();
+  const size_t per = wt_elems<M, OP>(g.S);
+  const size_t cap = p->scratch_bytes / sizeof(float2) / per;  // WTs that fit the scratch
+  if (p->schedule == SRK_SCHEDULE_PERSISTENT && cap >= 3) {
+    const int nslot = (int)std::min<size_t>({cap, (size_t)kMaxSlots, (size_t)(2 * kLag + 2)});
+    SRK_TRY(set_smem(k_persist<M, OP, T>, sm2));
+    int dev = 0, nsm = 0, per_sm = 0;
+    SRK_CUDA(cudaGetDevice(&dev));
+    SRK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    SRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<M, OP, T>, kThreads, sm2));
+    if (per_sm < 1) return fail(SRK_ERR_UNSUPPORTED, "persistent kernel does not fit an SM (smem %zu)", sm2);
+    const long long tickets = (long long)(nwt + 2 * kLag) * (M / kWarps * 2 + (g.S + kWarps - 1) / kWarps);
+    const int grid = (int)std::min<long long>((long long)nsm * per_sm, tickets);
+    SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
+    k_persist<M, OP, T><<<grid, kThreads, sm2, s>>>(a, g, p->G[0], p->G[1], conjG ? 1 : 0, p->tw, p->scratch, nslot,
+                                                   nwt, p->ctl, p->spin_limit);
+    SRK_CUDA(cudaGetLastError());
+    SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
+    p->mailbox_pending = true;
+    p->last_grid = grid;
+    p->last_launches = 1;
+    return SRK_OK;
+  }
   SRK_TRY(set_smem(k_p1<M, OP, T>, sm1));
   SRK_TRY(set_smem(k_p2<M, OP>, sm2));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
-  const size_t per_wt = (size_t)K * M * M;  // S1 elements per WT
-  float2* S1 = p->scratch;
-  float2* S2 = p->scratch + (size_t)p->chunk * per_wt;
-  for (int w0 = 0; w0 < nwt; w0 += p->chunk) {
-    const int c = (nwt - w0 < p->chunk) ? (nwt - w0) : p->chunk;
-    k_p1<M, OP, T><<<dim3(M / kWarps, K, c), kThreads, sm1, s>>>(a, g, p->tw, w0, S1);
-    k_p2<M, OP><<<dim3(M / kWarps, c), kThreads, sm2, s>>>(S1, S2, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
-    k_p3<M, OP, T><<<dim3((g.S + kWarps - 1) / kWarps, c), kThreads, sm3, s>>>(S2, a, g, p->tw, w0);
+  const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
+  int launches = 0;
+  for (int w0 = 0; w0 < nwt; w0 += chunk) {
+    const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
+    k_p1<M, OP, T><<<dim3(M / kWarps, c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
+    k_p2<M, OP><<<dim3(M / kWarps, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
+    k_p3<M, OP, T><<<dim3((g.S + kWarps - 1) / kWarps, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
+    launches += 3;
   }
+  p->last_launches = launches;
   return cuda_status(cudaGetLastError(), "conv launch");
 }
 
@@ -278,6 +308,28 @@ OpArgs base_args(const srk_plan_s* p) {
 
 srk_status set_device(const srk_plan_s* p) { return cuda_status(cudaSetDevice(p->device), "cudaSetDevice"); }
 
+// Report (once) a bounded wait that gave up in an already completed
+// persistent launch of this plan.
+srk_status check_mailbox(srk_plan_s* p) {
+  if (!p->mailbox_pending) return SRK_OK;
+  const cudaError_t q = cudaEventQuery(p->mailbox_ev);
+  if (q == cudaErrorNotReady) return SRK_OK;
+  if (q != cudaSuccess) return cuda_status(q, "mailbox event");
+  p->mailbox_pending = false;
+  if (p->mailbox[0]) {
+    const unsigned int where = p->mailbox[1];
+    p->mailbox[0] = 0;
+    return fail(SRK_ERR_TIMEOUT, "a bounded device-side wait gave up (site %u); that call's outputs are incomplete",
+                where);
+  }
+  return SRK_OK;
+}
+
+srk_status enter(srk_plan_s* p) {
+  SRK_TRY(set_device(p));
+  return check_mailbox(p);
+}
+
 // dL/dg through the adjoint engine: h = v*df (+ dv*f' for the tangent-adjoint)
 srk_status run_adj_g(srk_plan_s* p, const float* v, const float* dv, const float* f, const float* df, int B,
                      bool conj, float* out, cudaStream_t s) {
@@ -355,6 +407,14 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
       return cleanup(cuda_status(err, "spectrum allocation"));
   if ((err = cudaMalloc(reinterpret_cast<void**>(&p->tw), sizeof(float2) * M)) != cudaSuccess)
     return cleanup(cuda_status(err, "twiddle allocation"));
+  if ((err = cudaMalloc(reinterpret_cast<void**>(&p->ctl), sizeof(Ctl))) != cudaSuccess)
+    return cleanup(cuda_status(err, "control block allocation"));
+  if ((err = cudaHostAlloc(reinterpret_cast<void**>(&p->mailbox), 2 * sizeof(unsigned int), cudaHostAllocDefault)) !=
+      cudaSuccess)
+    return cleanup(cuda_status(err, "mailbox allocation"));
+  p->mailbox[0] = p->mailbox[1] = 0;
+  if ((err = cudaEventCreateWithFlags(&p->mailbox_ev, cudaEventDisableTiming)) != cudaSuccess)
+    return cleanup(cuda_status(err, "event creation"));
   std::vector<float2> tw(M);
   const std::vector<double2> t64 = twiddles64(M);
   for (int m = 0; m < M; ++m) tw[m] = make_float2((float)t64[m].x, (float)-t64[m].y);  // exp(-2 pi i m/M)
@@ -373,6 +433,9 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->G[1]) cudaFree(p->G[1]);
   if (p->tw) cudaFree(p->tw);
   if (p->wbuf) cudaFree(p->wbuf);
+  if (p->ctl) cudaFree(p->ctl);
+  if (p->mailbox) cudaFreeHost(p->mailbox);
+  if (p->mailbox_ev) cudaEventDestroy(p->mailbox_ev);
   delete p;
   return SRK_OK;
 }
@@ -382,7 +445,36 @@ srk_status srk_plan_get_info(srk_plan p, srk_plan_info* info) {
   info->N = p->N; info->W = p->W; info->erosion = p->e; info->B_max = p->B_max; info->spectra_M = p->spectra_M;
   info->dx = p->dx; info->tile_M = p->M; info->tile_stride = p->S; info->tiles = p->T; info->tiles_adj = p->Ta;
   info->chunk_wt = p->chunk; info->scratch_bytes = p->scratch_bytes; info->dtype = p->dtype;
+  info->schedule = p->schedule; info->last_launches = p->last_launches; info->last_grid = p->last_grid;
   return SRK_OK;
+}
+
+srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
+  if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
+  if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS)
+    return fail(SRK_ERR_INVALID_ARG, "bad schedule %d", (int)sch);
+  p->schedule = sch;
+  return SRK_OK;
+}
+
+srk_status srk_plan_sync(srk_plan p, srk_stream_t s) {
+  if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
+  SRK_TRY(set_device(p));
+  SRK_CUDA(cudaStreamSynchronize(s));
+  return check_mailbox(p);
+}
+
+srk_status srk_debug_wait_selftest(srk_plan p, unsigned long long spin_limit, srk_stream_t s) {
+  if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
+  if (spin_limit == 0 || spin_limit > (1ull << 26)) return fail(SRK_ERR_INVALID_ARG, "spin_limit out of range");
+  SRK_TRY(enter(p));
+  SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
+  k_wait_selftest<<<1, 32, 0, s>>>(p->ctl, spin_limit);
+  SRK_CUDA(cudaGetLastError());
+  SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
+  p->mailbox_pending = true;
+  return srk_plan_sync(p, s);
 }
 
 srk_status srk_plan_set_adj_convention(srk_plan p, srk_adj_convention c) {
@@ -450,7 +542,7 @@ srk_status srk_training_forward(const float* E, const float* I, const void* gx, 
   SRK_NONNULL(R);
   if (p->spectra_M != N && (gx || gy))
     return fail(SRK_ERR_INVALID_ARG, "training spectra must be at size N=%d (plan has spectra_M=%d)", N, p->spectra_M);
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R;
@@ -460,7 +552,7 @@ srk_status srk_training_forward(const float* E, const float* I, const void* gx, 
 srk_status srk_training_forward_sync(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
                                      int erosion, float dx, int B, srk_stream_t s, float* R, srk_plan p) {
   SRK_TRY(srk_training_forward(E, I, gx, gy, N, W, erosion, dx, B, s, R, p));
-  return cuda_status(cudaStreamSynchronize(s), "stream sync");
+  return srk_plan_sync(p, s);
 }
 
 srk_status srk_forward_oas(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
@@ -469,7 +561,7 @@ srk_status srk_forward_oas(const float* E, const float* I, const void* gx, const
   SRK_NONNULL(E);
   SRK_NONNULL(I);
   SRK_NONNULL(R);
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R; a.out_ux = ux; a.out_uy = uy;
@@ -486,7 +578,7 @@ srk_status srk_adjoint(const float* v, const float* ux, const float* uy, const f
   SRK_NONNULL(I);
   SRK_NONNULL(dLdI);
   SRK_NONNULL(dLdE);
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   SRK_TRY(adj_wrt_f(p, nullptr, nullptr, v, ux, uy, 1, dLdI, s));
   return run_adj_g(p, v, nullptr, I, nullptr, 1, p->conv == SRK_ADJ_TRUE, dLdE, s);
@@ -500,7 +592,7 @@ srk_status srk_tangent(const float* f, const float* g, const float* df, const fl
   SRK_NONNULL(df);
   SRK_NONNULL(dg);
   SRK_NONNULL(dh);
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
@@ -519,7 +611,7 @@ srk_status srk_tangent_adjoint(const float* f, const float* g, const float* df, 
   SRK_NONNULL(dlam);
   SRK_NONNULL(dLam_f);
   SRK_NONNULL(dLam_g);
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   const size_t ww = (size_t)p->W * p->W;
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
@@ -537,7 +629,7 @@ srk_status srk_forward(const float* f, const float* g, int B, srk_stream_t s, fl
   SRK_NONNULL(g);
   SRK_NONNULL(h);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   OpArgs a = base_args(p);
   a.E = g; a.I = f; a.out0 = h;
   return launch_conv<OP_FWD, float>(p, a, fwd_geom(p, B), false, s);
@@ -553,7 +645,7 @@ srk_status srk_vjp(const float* v, const float* f, const float* g, int B, srk_st
   SRK_NONNULL(dLdf);
   SRK_NONNULL(dLdg);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   const size_t ww = (size_t)p->W * p->W * B;
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
   OpArgs a = base_args(p);
@@ -574,7 +666,7 @@ srk_status srk_jvp(const float* f, const float* g, const float* df, const float*
   SRK_NONNULL(dg);
   SRK_NONNULL(dh);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(set_device(p));
+  SRK_TRY(enter(p));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
   return launch_conv<OP_JVP, float>(p, a, fwd_geom(p, B), false, s);

@@ -229,3 +229,44 @@ def test_error_paths_on_device(torch_cuda):
     with pytest.raises(srk.SrkError) as ei:   # size mismatch with the plan
         srk.srkTrainingForward(E, E, None, None, 128, 96, 16, 1.0, 2, None, R, plan)
     assert ei.value.status == srk.SRK_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("N,KW,B,tile", [(256, 31, 7, 0), (512, 121, 3, 0), (300, 31, 2, 128)])
+def test_persistent_and_three_pass_schedules_agree(torch_cuda, N, KW, B, tile):
+    """Both kernel schedules run the same phases on the same work tiles: the
+    results must be bit-identical, and match the oracle."""
+    torch = torch_cuda
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    Kx, Ky = kernel(KW)
+    GX, GY = spectra(Kx, Ky, N, torch)
+    E = dev(np.stack(fields(N, B, 40 + N)), torch)
+    out = []
+    for sch in (srk.SRK_SCHEDULE_PERSISTENT, srk.SRK_SCHEDULE_THREE_PASS):
+        plan = srk.SrkPlan(N, W, e, 1.0, B, tile_M=tile)
+        plan.set_schedule(sch)
+        R = torch.zeros((B, W, W), device="cuda")
+        srk.srkTrainingForward(E, E, GX, GY, N, W, e, 1.0, B, None, R, plan)
+        plan.sync()
+        launches = plan.info()["last_launches"]
+        assert launches == 1 if sch == srk.SRK_SCHEDULE_PERSISTENT else launches % 3 == 0
+        out.append(host(R))
+    assert np.array_equal(out[0], out[1])
+    Eh = host(E)
+    for b in range(B):
+        assert rel_max_err(out[0][b], O.forward(Eh[b], Eh[b], Kx, Ky, e, 1.0)) < 1e-3
+
+
+def test_bounded_wait_gives_up_and_context_survives(torch_cuda):
+    torch = torch_cuda
+    plan = srk.SrkPlan(128, 98, 15, 1.0, 2)
+    assert plan.wait_selftest(1 << 12) == srk.SRK_ERR_TIMEOUT
+    assert b"bounded" in srk.lib().srk_last_error()
+    # the context is still usable: a normal call afterwards succeeds
+    Kx, Ky = kernel(31)
+    GX, GY = spectra(Kx, Ky, 128, torch)
+    E = dev(np.stack(fields(128, 2, 5)), torch)
+    R = torch.zeros((2, 98, 98), device="cuda")
+    srk.srkTrainingForward(E, E, GX, GY, 128, 98, 15, 1.0, 2, None, R, plan)
+    plan.sync()
+    assert rel_max_err(host(R)[0], O.forward(host(E)[0], host(E)[0], Kx, Ky, 15, 1.0)) < 1e-3
