@@ -72,6 +72,9 @@ typedef struct srk_plan_info {
   int schedule;       /* srk_schedule */
   int last_launches;  /* kernel launches of the last engine call */
   int last_grid;      /* CTAs of the last persistent launch */
+  int last_lag;       /* rounds between phases in the last persistent launch */
+  int last_nslot;     /* scratch ring slots of the last persistent launch */
+  unsigned long long last_spins; /* dependency polls that found work not ready (completed launches) */
 } srk_plan_info;
 
 /* ---- library ------------------------------------------------------------ */
@@ -94,6 +97,10 @@ srk_status srk_plan_destroy(srk_plan plan);
 srk_status srk_plan_get_info(srk_plan plan, srk_plan_info* info);
 srk_status srk_plan_set_adj_convention(srk_plan plan, srk_adj_convention conv);
 srk_status srk_plan_set_schedule(srk_plan plan, srk_schedule schedule);
+/* Persistent-schedule tuning: lag (rounds between the phases of a work
+ * tile; 0 = derived from the grid), grid (CTAs; 0 = all that fit), prefetch
+ * (1 = fetch the next ticket while running the current one). */
+srk_status srk_plan_set_persistent(srk_plan plan, int lag, int grid, int prefetch);
 /* Synchronise `stream` and report a device-side failure of the plan's last
  * persistent launch (SRK_ERR_TIMEOUT if a bounded wait gave up).  Operators
  * also report such a failure of the previous call once it has completed. */

@@ -23,7 +23,7 @@ __all__ = [
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libsrk_b200.so")
+LIB_PATH = os.environ.get("SRK_B200_LIB") or os.path.join(_PKG, "libsrk_b200.so")
 
 SRK_OK, SRK_ERR_INVALID_ARG, SRK_ERR_UNSUPPORTED, SRK_ERR_ALLOC, SRK_ERR_TIMEOUT, SRK_ERR_CUDA = range(6)
 SRK_F32, SRK_F16, SRK_BF16 = 0, 1, 2
@@ -46,7 +46,8 @@ class PlanInfo(ctypes.Structure):
                 ("spectra_M", ctypes.c_int), ("dx", ctypes.c_float), ("tile_M", ctypes.c_int),
                 ("tile_stride", ctypes.c_int), ("tiles", ctypes.c_int), ("tiles_adj", ctypes.c_int),
                 ("chunk_wt", ctypes.c_int), ("scratch_bytes", ctypes.c_size_t), ("dtype", ctypes.c_int),
-                ("schedule", ctypes.c_int), ("last_launches", ctypes.c_int), ("last_grid", ctypes.c_int)]
+                ("schedule", ctypes.c_int), ("last_launches", ctypes.c_int), ("last_grid", ctypes.c_int),
+                ("last_lag", ctypes.c_int), ("last_nslot", ctypes.c_int), ("last_spins", ctypes.c_ulonglong)]
 
 
 _lib = None
@@ -65,6 +66,7 @@ _SIGS = {
     "srk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "srk_plan_set_adj_convention": [_P, _I],
     "srk_plan_set_schedule": [_P, _I],
+    "srk_plan_set_persistent": [_P, _I, _I, _I],
     "srk_plan_sync": [_P, _P],
     "srk_debug_wait_selftest": [_P, ctypes.c_ulonglong, _P],
     "srk_plan_import_spectra": [_P, _P, _P, _P],
@@ -149,6 +151,9 @@ class SrkPlan:
 
     def set_schedule(self, schedule):
         _check(lib().srk_plan_set_schedule(self.handle, schedule))
+
+    def set_persistent(self, lag=0, grid=0, prefetch=1):
+        _check(lib().srk_plan_set_persistent(self.handle, lag, grid, prefetch))
 
     def sync(self, stream=None):
         """Synchronise and raise SrkError(SRK_ERR_TIMEOUT) if a bounded

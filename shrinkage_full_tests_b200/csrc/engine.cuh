@@ -35,6 +35,11 @@
 #include <cstdint>
 #include "fft_warp.cuh"
 
+// CTAs per SM the kernels are compiled for (register cap 65536/(256*n)).
+#ifndef SRK_MIN_BLOCKS
+#define SRK_MIN_BLOCKS 3
+#endif
+
 namespace srk {
 
 enum Op : int {
@@ -154,36 +159,96 @@ __device__ __forceinline__ float h_at(const OpArgs& a, int b, int k, int px, int
   return dv * g + v * dg;
 }
 
+// Column x of one real tile of image `img` (forward-type ops): values at
+// rows y = lane + 32 i, zero outside the image.  Pointers are hoisted so the
+// loads are (base + immediate); bounds are tested per element only for a
+// tile that crosses the bottom edge.
+template <int M, typename T>
+__device__ __forceinline__ void load_tile_column(const T* __restrict__ img, int N, const TileRef& t, int x, int lane,
+                                                 float (&v)[M / 32]) {
+  constexpr int EPT = M / 32;
+  const int gx = t.x0 + x;
+  if (!t.live || gx >= N) {
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) v[i] = 0.f;
+    return;
+  }
+  const T* col = img + (long long)t.b * N * N + (long long)gx * N + t.y0 + lane;
+  const int rows = N - t.y0 - lane;  // rows available below this lane's first element
+  if (N - t.y0 >= M) {
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) v[i] = ldf(col, 32 * i);
+  } else {
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) v[i] = (32 * i < rows) ? ldf(col, 32 * i) : 0.f;
+  }
+}
+
 template <int M, int OP, typename T>
 __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int w, int k, int x, int lane,
                                             float2 (&z)[M / 32]) {
   constexpr int EPT = M / 32;
-  if constexpr (OpTraits<OP>::PAIRS) {
+  if constexpr (OP == OP_ADJ) {
     const TileRef t0 = tile_of(g, 2 * w), t1 = tile_of(g, 2 * w + 1);
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       const int y = lane + 32 * i;
-      float re = 0.f, im = 0.f;
-      if constexpr (OP == OP_ADJ) {
-        re = h_at<T>(a, t0.b, k, t0.x0 + x, t0.y0 + y);
-        if (t1.live) im = h_at<T>(a, t1.b, k, t1.x0 + x, t1.y0 + y);
-      } else {
-        const T* E = static_cast<const T*>(a.E);
-        re = img_at(E, a, t0.b, t0.x0 + x, t0.y0 + y);
-        if (t1.live) im = img_at(E, a, t1.b, t1.x0 + x, t1.y0 + y);
-      }
+      const float re = h_at<T>(a, t0.b, k, t0.x0 + x, t0.y0 + y);
+      const float im = t1.live ? h_at<T>(a, t1.b, k, t1.x0 + x, t1.y0 + y) : 0.f;
       z[i] = make_float2(re, im);
     }
-  } else {
-    const TileRef t = tile_of(g, w);
+  } else if constexpr (OpTraits<OP>::PAIRS) {
+    float re[EPT], im[EPT];
     const T* E = static_cast<const T*>(a.E);
-    const T* dE = static_cast<const T*>(a.dE);
+    load_tile_column<M, T>(E, a.N, tile_of(g, 2 * w), x, lane, re);
+    load_tile_column<M, T>(E, a.N, tile_of(g, 2 * w + 1), x, lane, im);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int y = lane + 32 * i;
-      z[i] = make_float2(img_at(E, a, t.b, t.x0 + x, t.y0 + y), img_at(dE, a, t.b, t.x0 + x, t.y0 + y));
+    for (int i = 0; i < EPT; ++i) z[i] = make_float2(re[i], im[i]);
+  } else {
+    float re[EPT], im[EPT];
+    const TileRef t = tile_of(g, w);
+    load_tile_column<M, T>(static_cast<const T*>(a.E), a.N, t, x, lane, re);
+    load_tile_column<M, T>(static_cast<const T*>(a.dE), a.N, t, x, lane, im);
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) z[i] = make_float2(re[i], im[i]);
+  }
+}
+
+// Central differences of f at image column gx for this lane's rows
+// gy = gy0 + 32 i: fx = (f[gx+1] - f[gx-1])/2, fy = (f[gy+1] - f[gy-1])/2.
+// With erosion >= 1 every valid output has its 4 neighbours inside the
+// image, so the zero-padding rule of srk_grad_x/_y never applies and the
+// loads need no test; erosion 0 takes the tested path.
+template <typename T>
+struct GradCol {
+  const T* c;   // f + gx*N + gy0
+  int N;
+  bool tested;
+  int gx, gy0;
+  __device__ __forceinline__ void at(int i, float& fx, float& fy) const {
+    if (!tested) {
+      fx = (ldf(c + N, 32 * i) - ldf(c - N, 32 * i)) * 0.5f;
+      fy = (ldf(c + 1, 32 * i) - ldf(c - 1, 32 * i)) * 0.5f;
+    } else {
+      const int gy = gy0 + 32 * i;
+      const float r = (gx + 1 < N) ? ldf(c + N, 32 * i) : 0.f;
+      const float l = (gx > 0) ? ldf(c - N, 32 * i) : 0.f;
+      const float d = (gy + 1 < N) ? ldf(c + 1, 32 * i) : 0.f;
+      const float u = (gy > 0) ? ldf(c - 1, 32 * i) : 0.f;
+      fx = (r - l) * 0.5f;
+      fy = (d - u) * 0.5f;
     }
   }
+};
+template <typename T>
+__device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int gx, int gy0) {
+  GradCol<T> gc;
+  gc.c = f_img + (long long)gx * N + gy0;
+  gc.N = N;
+  gc.tested = e < 1;
+  gc.gx = gx;
+  gc.gy0 = gy0;
+  return gc;
 }
 
 // ---- epilogues: P3 hands over column x (local, valid) of work tile w ------
@@ -193,79 +258,93 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
                                                 const float2 (&z0)[M / 32], const float2 (&z1)[M / 32]) {
   constexpr int EPT = M / 32;
   const int N = a.N, W = a.W, e = a.e;
-  auto emit_fwd = [&](const TileRef& t, bool imag) {
-    if (!t.live) return;
-    const int ox = t.x0 + x - g.e;
-    if (ox >= g.Wout) return;
-    const T* f = static_cast<const T*>(a.I) + (long long)t.b * N * N;
-    const long long ob = (long long)t.b * W * W + (long long)ox * W;
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int y = lane + 32 * i;
-      const int oy = t.y0 + y - g.e;
-      if (y < g.e || y >= g.e + g.S || oy >= g.Wout) continue;
-      const float ux = imag ? z0[i].y : z0[i].x;
-      const float uy = imag ? z1[i].y : z1[i].x;
-      const int gx = ox + e, gy = oy + e;
-      if constexpr (OP == OP_FWD) {
-        if (a.out0) {
-          const float r = ux * grad_x(f, N, gx, gy) + uy * grad_y(f, N, gx, gy);
-          stf(static_cast<T*>(a.out0), ob + oy, r);
-        }
-        if (a.out_ux) stf(static_cast<T*>(a.out_ux), ob + oy, ux);
-        if (a.out_uy) stf(static_cast<T*>(a.out_uy), ob + oy, uy);
-      } else {  // OP_VJP_F: w = u * v
-        const float v = ldf(static_cast<const T*>(a.v), ob + oy);
-        stf(static_cast<float*>(a.out0), ob + oy, ux * v);
-        stf(static_cast<float*>(a.out1), ob + oy, uy * v);
-      }
-    }
+  // rows handled by this lane: y = lane + 32 i valid iff y in [e, e+S) and
+  // its output row y0 + y - e < Wout
+  auto valid_row = [&](const TileRef& t, int i) {
+    const int y = lane + 32 * i;
+    return y >= g.e && y < g.e + g.S && t.y0 + y - g.e < g.Wout;
   };
   if constexpr (OP == OP_FWD || OP == OP_VJP_F) {
-    emit_fwd(tile_of(g, 2 * w), false);
-    emit_fwd(tile_of(g, 2 * w + 1), true);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const TileRef t = tile_of(g, 2 * w + h);
+      const int ox = t.x0 + x - g.e;
+      if (!t.live || ox >= g.Wout) continue;
+      // output row oy = y0 + y - e  ->  pointer to row (y0 - e + lane)
+      const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+      if constexpr (OP == OP_FWD) {
+        const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e,
+                                       t.y0 + lane);
+        T* R = static_cast<T*>(a.out0);
+        T* UX = static_cast<T*>(a.out_ux);
+        T* UY = static_cast<T*>(a.out_uy);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          if (!valid_row(t, i)) continue;
+          const float ux = h ? z0[i].y : z0[i].x;
+          const float uy = h ? z1[i].y : z1[i].x;
+          if (R) {
+            float fx, fy;
+            gc.at(i, fx, fy);
+            stf(R, ob + 32 * i, ux * fx + uy * fy);
+          }
+          if (UX) stf(UX, ob + 32 * i, ux);
+          if (UY) stf(UY, ob + 32 * i, uy);
+        }
+      } else {  // OP_VJP_F: w = u * v
+        const T* V = static_cast<const T*>(a.v);
+        float* WX = static_cast<float*>(a.out0);
+        float* WY = static_cast<float*>(a.out1);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+          if (!valid_row(t, i)) continue;
+          const float v = ldf(V, ob + 32 * i);
+          WX[ob + 32 * i] = (h ? z0[i].y : z0[i].x) * v;
+          WY[ob + 32 * i] = (h ? z1[i].y : z1[i].x) * v;
+        }
+      }
+    }
   } else if constexpr (OP == OP_JVP || OP == OP_TANADJ_F) {
     const TileRef t = tile_of(g, w);
     const int ox = t.x0 + x - g.e;
     if (ox >= g.Wout) return;
-    const long long ob = (long long)t.b * W * W + (long long)ox * W;
+    const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+    if constexpr (OP == OP_JVP) {
+      // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52); re: conv of g, im: conv of dg
+      const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
+      const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int y = lane + 32 * i;
-      const int oy = t.y0 + y - g.e;
-      if (y < g.e || y >= g.e + g.S || oy >= g.Wout) continue;
-      // re: conv of g, im: conv of dg
-      if constexpr (OP == OP_JVP) {
-        const T* f = static_cast<const T*>(a.I) + (long long)t.b * N * N;
-        const T* df = static_cast<const T*>(a.dI) + (long long)t.b * N * N;
-        const int gx = ox + e, gy = oy + e;
-        // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52)
-        const float dh = z0[i].y * grad_x(f, N, gx, gy) + z1[i].y * grad_y(f, N, gx, gy) +
-                         z0[i].x * grad_x(df, N, gx, gy) + z1[i].x * grad_y(df, N, gx, gy);
-        stf(static_cast<T*>(a.out0), ob + oy, dh);
-      } else {
-        const float lam = ldf(static_cast<const T*>(a.v), ob + oy);
-        const float dlam = ldf(static_cast<const T*>(a.dv), ob + oy);
-        stf(static_cast<float*>(a.out0), ob + oy, dlam * z0[i].x + lam * z0[i].y);
-        stf(static_cast<float*>(a.out1), ob + oy, dlam * z1[i].x + lam * z1[i].y);
+      for (int i = 0; i < EPT; ++i) {
+        if (!valid_row(t, i)) continue;
+        float fx, fy, dfx, dfy;
+        gf.at(i, fx, fy);
+        gd.at(i, dfx, dfy);
+        stf(static_cast<T*>(a.out0), ob + 32 * i, z0[i].y * fx + z1[i].y * fy + z0[i].x * dfx + z1[i].x * dfy);
+      }
+    } else {
+      const T* LAM = static_cast<const T*>(a.v);
+      const T* DLAM = static_cast<const T*>(a.dv);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        if (!valid_row(t, i)) continue;
+        const float lam = ldf(LAM, ob + 32 * i), dlam = ldf(DLAM, ob + 32 * i);
+        static_cast<float*>(a.out0)[ob + 32 * i] = dlam * z0[i].x + lam * z0[i].y;
+        static_cast<float*>(a.out1)[ob + 32 * i] = dlam * z1[i].x + lam * z1[i].y;
       }
     }
   } else {  // OP_ADJ: output is the full N x N image
-    auto emit_adj = [&](const TileRef& t, bool imag) {
-      if (!t.live) return;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const TileRef t = tile_of(g, 2 * w + h);
       const int ox = t.x0 + x - g.e;
-      if (ox >= g.Wout) return;
-      const long long ob = (long long)t.b * N * N + (long long)ox * N;
+      if (!t.live || ox >= g.Wout) continue;
+      const long long ob = (long long)t.b * N * N + (long long)ox * N + t.y0 - g.e + lane;
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
-        const int y = lane + 32 * i;
-        const int oy = t.y0 + y - g.e;
-        if (y < g.e || y >= g.e + g.S || oy >= g.Wout) continue;
-        stf(static_cast<T*>(a.out0), ob + oy, imag ? z0[i].y : z0[i].x);
+        if (!valid_row(t, i)) continue;
+        stf(static_cast<T*>(a.out0), ob + 32 * i, h ? z0[i].y : z0[i].x);
       }
-    };
-    emit_adj(tile_of(g, 2 * w), false);
-    emit_adj(tile_of(g, 2 * w + 1), true);
+    }
   }
 }
 
@@ -277,18 +356,37 @@ __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restri
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
 }
 
-// Scratch of one work tile: S1 [K][M][M] then S2 [L][S][M] (float2).
+// Staging rows: stride RW + 2 float2 so that the 8 rows of a transposing
+// copy fall into different banks.
+template <int M>
+__host__ __device__ constexpr int row_stride() { return fft_row_words(M) + 2; }
+// S2 rows are padded to a multiple of 8 columns (16-byte aligned float4 reads).
+__host__ __device__ inline int s2_pitch(int S) { return (S + 7) & ~7; }
+
+// Scratch of one work tile: S1 [K][x < M][ky < M] then S2 [L][ky < M][x' < pitch(S)] (float2).
 template <int M, int OP>
 __host__ __device__ constexpr size_t s1_elems() { return (size_t)OpTraits<OP>::K * M * M; }
 template <int M, int OP>
-__host__ __device__ inline size_t wt_elems(int S) { return s1_elems<M, OP>() + (size_t)OpTraits<OP>::L * S * M; }
+__host__ __device__ inline size_t wt_elems(int S) {
+  return s1_elems<M, OP>() + (size_t)OpTraits<OP>::L * M * s2_pitch(S);
+}
 
+// Shared memory of every phase: the twiddle table and 2 x 8 staging rows.
 template <int M>
-constexpr size_t p1_smem_bytes() { return sizeof(float2) * (M + kWarps * fft_row_words(M)); }
+constexpr size_t phase_smem_bytes() { return sizeof(float2) * (M + 2 * kWarps * row_stride<M>()); }
+
+// Warp-wide copy between registers (strided order) and a padded row.
 template <int M>
-constexpr size_t p3_smem_bytes() { return p1_smem_bytes<M>(); }
-inline size_t p2_smem_bytes(int M, int K, int L, int S) {
-  return sizeof(float2) * ((size_t)M + (size_t)K * kWarps * fft_row_words(M) + (size_t)L * S * 9);
+__device__ __forceinline__ void row_to_regs(const float2* __restrict__ row, float2 (&z)[M / 32], int lane) {
+  const float2* rd = row + lane + (lane >> 4);
+#pragma unroll
+  for (int i = 0; i < M / 32; ++i) z[i] = rd[34 * i];
+}
+template <int M>
+__device__ __forceinline__ void regs_to_row(float2* __restrict__ row, const float2 (&z)[M / 32], int lane) {
+  float2* wr = row + lane + (lane >> 4);
+#pragma unroll
+  for (int i = 0; i < M / 32; ++i) wr[34 * i] = z[i];
 }
 
 // P1: warp `warp` transforms column x = xb*8 + warp of every field along y.
@@ -309,101 +407,116 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
   }
 }
 
-// P2: rows ky0 .. ky0+7: FFT along x, spectral map, inverse, keep the valid
-// columns, write S2 column-contiguous through a padded transpose buffer.
-// Needs __syncthreads-uniform control flow (all threads of the CTA).
-template <int M, int OP>
-__device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __restrict__ S2,
-                                       const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
-                                       const Geom& g, int ky0, float2* __restrict__ buf,
-                                       const float2* __restrict__ tw, int warp, int lane) {
-  constexpr int EPT = M / 32;
-  constexpr int K = OpTraits<OP>::K;
-  constexpr int L = OpTraits<OP>::L;
-  constexpr int RW = fft_row_words(M);
-  float2* in = buf;                      // [K][8][RW]
-  float2* out = buf + K * kWarps * RW;   // [L][S][9]
-  const int S = g.S, e = g.e;
-  for (int idx = threadIdx.x; idx < K * M * 4; idx += kThreads) {
-    const int k = idx / (M * 4);
-    const int rem = idx - k * (M * 4);
-    const int x = rem >> 2, rp = rem & 3;
-    const float4 q = __ldcg(reinterpret_cast<const float4*>(S1 + ((size_t)k * M + x) * M + ky0 + 2 * rp));
-    in[(k * kWarps + 2 * rp) * RW + fft_pad(x)] = make_float2(q.x, q.y);
-    in[(k * kWarps + 2 * rp + 1) * RW + fft_pad(x)] = make_float2(q.z, q.w);
-  }
-  __syncthreads();
-  const int ky = ky0 + warp;
-  float2* row0 = in + warp * RW;
-  const float2* rd0 = row0 + lane + (lane >> 4);
-  float2 z0[EPT];
-#pragma unroll
-  for (int i = 0; i < EPT; ++i) z0[i] = rd0[34 * i];
-  fft<M, false>(z0, row0, tw, lane);
-  const float2* gxr = Gx + (size_t)ky * M + lane;
-  const float2* gyr = Gy + (size_t)ky * M + lane;
-  auto spec = [&](float2 z, float2 G) { return conjG ? cmulc(z, G) : cmul(z, G); };
-  auto park = [&](const float2 (&o)[EPT], int l) {
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int xv = lane + 32 * i - e;
-      if (xv >= 0 && xv < S) out[(l * S + xv) * 9 + warp] = o[i];
-    }
-  };
-  if constexpr (K == 1) {
-    float2 o[EPT];
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gxr + 32 * i));
-    fft<M, true>(o, row0, tw, lane);
-    park(o, 0);
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) o[i] = spec(z0[i], __ldg(gyr + 32 * i));
-    fft<M, true>(o, row0, tw, lane);
-    park(o, 1);
-  } else {
-    float2* row1 = in + (kWarps + warp) * RW;
-    const float2* rd1 = row1 + lane + (lane >> 4);
-    float2 z1[EPT];
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) z1[i] = rd1[34 * i];
-    fft<M, false>(z1, row1, tw, lane);
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) z0[i] = cadd(spec(z0[i], __ldg(gxr + 32 * i)), spec(z1[i], __ldg(gyr + 32 * i)));
-    fft<M, true>(z0, row0, tw, lane);
-    park(z0, 0);
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < L * S * 4; idx += kThreads) {
-    const int l = idx / (S * 4);
-    const int rem = idx - l * (S * 4);
-    const int xv = rem >> 2, rp = rem & 3;
-    const float2 lo = out[(l * S + xv) * 9 + 2 * rp];
-    const float2 hi = out[(l * S + xv) * 9 + 2 * rp + 1];
-    __stcg(reinterpret_cast<float4*>(S2 + ((size_t)l * S + xv) * M + ky0 + 2 * rp),
-           make_float4(lo.x, lo.y, hi.x, hi.y));
+// Transposing copy: 8 consecutive columns [c0, c0+8) of a column-contiguous
+// block (column pitch `pitch`, M rows) into 8 staging rows, one per column.
+// Columns >= ncol are not read.  All threads of the CTA take part.
+template <int M>
+__device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int pitch, int ncol,
+                                           float2* __restrict__ rows) {
+  constexpr int RS = row_stride<M>();
+  for (int idx = threadIdx.x; idx < M * 4; idx += kThreads) {
+    const int y = idx >> 2, cp = idx & 3;
+    if (2 * cp >= ncol) continue;
+    const float4 q = __ldcg(reinterpret_cast<const float4*>(src + (size_t)y * pitch + 2 * cp));
+    rows[(2 * cp) * RS + fft_pad(y)] = make_float2(q.x, q.y);
+    rows[(2 * cp + 1) * RS + fft_pad(y)] = make_float2(q.z, q.w);
   }
 }
 
-// P3: warp `warp` finishes valid column xv = xb*8 + warp (if < S).
+// P2: rows ky0 .. ky0+7: FFT along x, spectral map, inverse, keep the valid
+// columns, write S2 rows.  All threads of the CTA take part.
+template <int M, int OP>
+__device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __restrict__ S2,
+                                       const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
+                                       const Geom& g, int ky0, float2* __restrict__ rows,
+                                       const float2* __restrict__ tw, int warp, int lane) {
+  constexpr int EPT = M / 32;
+  constexpr int K = OpTraits<OP>::K;
+  constexpr int RS = row_stride<M>();
+  const int S = g.S, e = g.e, P = s2_pitch(S);
+  // S1 viewed as rows ky (pitch M) of columns x: a transposing copy of the
+  // 8 columns ky0.. of the (x, ky) matrix -- i.e. S1[k][x][ky0 + c].
+  for (int k = 0; k < K; ++k) {
+    const float2* src = S1 + (size_t)k * M * M + ky0;
+    float2* dst = rows + k * kWarps * RS;
+    for (int idx = threadIdx.x; idx < M * 4; idx += kThreads) {
+      const int x = idx >> 2, rp = idx & 3;
+      const float4 q = __ldcg(reinterpret_cast<const float4*>(src + (size_t)x * M + 2 * rp));
+      dst[(2 * rp) * RS + fft_pad(x)] = make_float2(q.x, q.y);
+      dst[(2 * rp + 1) * RS + fft_pad(x)] = make_float2(q.z, q.w);
+    }
+  }
+  __syncthreads();
+  const int ky = ky0 + warp;
+  float2* row0 = rows + warp * RS;              // field 0 / exchange
+  float2* row1 = rows + (kWarps + warp) * RS;   // field 1 or the stash
+  const float2* gxr = Gx + (size_t)ky * M + lane;
+  const float2* gyr = Gy + (size_t)ky * M + lane;
+  auto spec = [&](float2 z, float2 G) { return conjG ? cmulc(z, G) : cmul(z, G); };
+  auto emit = [&](const float2 (&o)[EPT], int l) {
+    float2* dst = S2 + ((size_t)l * M + ky) * P - e + lane;
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const int xv = lane + 32 * i - e;
+      if (xv >= 0 && xv < S) __stcg(dst + 32 * i, o[i]);
+    }
+  };
+  float2 z[EPT];
+  row_to_regs<M>(row0, z, lane);
+  fft<M, false>(z, row0, tw, lane);
+  if constexpr (K == 1) {
+    regs_to_row<M>(row1, z, lane);  // stash Z(ky, .)
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const float2* gr = l ? gyr : gxr;
+      const float2* st = row1 + lane + (lane >> 4);
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) z[i] = spec(st[34 * i], __ldg(gr + 32 * i));
+      fft<M, true>(z, row0, tw, lane);
+      emit(z, 0 + l);
+    }
+  } else {
+    __syncwarp();
+    regs_to_row<M>(row0, z, lane);  // stash Z0(ky, .) in its own row
+    row_to_regs<M>(row1, z, lane);
+    fft<M, false>(z, row1, tw, lane);
+    const float2* st = row0 + lane + (lane >> 4);
+#pragma unroll
+    for (int i = 0; i < EPT; ++i)
+      z[i] = cadd(spec(st[34 * i], __ldg(gxr + 32 * i)), spec(z[i], __ldg(gyr + 32 * i)));
+    fft<M, true>(z, row1, tw, lane);
+    emit(z, 0);
+  }
+}
+
+// P3: columns x' = xb*8 .. +7: stage them, inverse FFT along ky, epilogue.
+// All threads of the CTA take part.
 template <int M, int OP, typename T>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
-                                       float2* __restrict__ row, const float2* __restrict__ tw, int warp, int lane) {
+                                       float2* __restrict__ rows, const float2* __restrict__ tw, int warp,
+                                       int lane) {
   constexpr int EPT = M / 32;
   constexpr int L = OpTraits<OP>::L;
-  const int xv = xb * kWarps + warp;
+  constexpr int RS = row_stride<M>();
+  const int P = s2_pitch(g.S);
+  const int x0 = xb * kWarps;
+  for (int l = 0; l < L; ++l)
+    stage_rows<M>(S2 + (size_t)l * M * P + x0, P, P - x0, rows + l * kWarps * RS);
+  __syncthreads();
+  const int xv = x0 + warp;
   if (xv >= g.S) return;
+  float2* row0 = rows + warp * RS;
+  float2* row1 = rows + (kWarps + warp) * RS;
   float2 z0[EPT], z1[EPT];
-  {
-    const float2* src = S2 + (size_t)xv * M + lane;
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) z0[i] = __ldcg(src + 32 * i);
-    fft<M, true>(z0, row, tw, lane);
-  }
+  row_to_regs<M>(row0, z0, lane);
+  fft<M, true>(z0, row0, tw, lane);
   if constexpr (L == 2) {
-    const float2* src = S2 + ((size_t)g.S + xv) * M + lane;
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) z1[i] = __ldcg(src + 32 * i);
-    fft<M, true>(z1, row, tw, lane);
+    __syncwarp();
+    regs_to_row<M>(row0, z0, lane);   // stash, reload after the second transform
+    row_to_regs<M>(row1, z1, lane);
+    fft<M, true>(z1, row1, tw, lane);
+    __syncwarp();
+    row_to_regs<M>(row0, z0, lane);
   } else {
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z1[i] = make_float2(0.f, 0.f);
@@ -413,19 +526,19 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
 
 // ---- three-launch schedule (one kernel per phase over a chunk of WTs) ------
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
   extern __shared__ float2 sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(sm, twg, M);
   __syncthreads();
   const int wl = blockIdx.y;
-  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + warp * fft_row_words(M),
+  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + warp * row_stride<M>(),
                    sm, warp, lane);
 }
 
 template <int M, int OP>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG, Geom g,
      const float2* __restrict__ twg) {
   extern __shared__ float2 sm[];
@@ -436,21 +549,20 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
 }
 
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
   extern __shared__ float2 sm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   load_twiddles(sm, twg, M);
-  __syncthreads();
   const int wl = blockIdx.y;
-  phase3<M, OP, T>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
-                   sm + M + warp * fft_row_words(M), sm, warp, lane);
+  phase3<M, OP, T>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x, sm + M, sm,
+                   warp, lane);
 }
 
 // ---- persistent schedule ---------------------------------------------------------
 // One launch processes every WT.  Work is a ticket queue of rounds; round r
-// holds the P1 units of WT r, the P2 units of WT r-kLag and the P3 units of
-// WT r-2*kLag.  A WT's scratch lives in slot w mod nslot of a small ring that
+// holds the P1 units of WT r, the P2 units of WT r-lag and the P3 units of
+// WT r-2*lag.  A WT's scratch lives in slot w mod nslot of a small ring that
 // stays in L2.  Per-slot counters (monotonic over the slot's reuses) order
 // the phases:
 //   P1(w) needs c2[slot] >= gen*n2       (previous user's P2 done reading S1)
@@ -458,18 +570,29 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
 //           and c3[slot] >= gen*n3       (previous user's P3 done reading S2)
 //   P3(w) needs c2[slot] >= (gen+1)*n2   (its S2 complete)
 // Every dependency points to a smaller ticket, and a ticket is only ever held
-// by a running CTA, so the smallest unfinished ticket can always proceed.
-// Waits are bounded anyway: a wait that exceeds `spin_limit` polls sets
-// ctl->abort (with the place in ctl->where) and every CTA returns.
-constexpr int kLag = 2;
-constexpr int kMaxSlots = 16;
+// by a running CTA (a CTA holds at most its current ticket and one
+// prefetched larger one), so the smallest unfinished ticket can always
+// proceed.  The lag and the ring size only decide how often a unit finds its
+// dependency not yet met.  Waits are bounded anyway: a wait that exceeds
+// `spin_limit` polls sets ctl->abort (with the place in ctl->where) and every
+// CTA returns.
+constexpr int kMaxSlots = 32;
 
 struct Ctl {
   unsigned int ticket;
   unsigned int abort;
   unsigned int where;
   unsigned int pad;
+  unsigned long long spins;  // polls that found a dependency unmet (diagnostic)
   unsigned int c1[kMaxSlots], c2[kMaxSlots], c3[kMaxSlots];
+};
+
+struct PersistParams {
+  int lag;        // rounds between the phases of one WT
+  int nslot;      // scratch ring slots (> lag)
+  int prefetch;   // fetch the next ticket while running the current one
+  int pad;
+  unsigned long long spin_limit;
 };
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
@@ -480,7 +603,7 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
 
 // Thread-0 wait: returns false if the kernel must stop.
 __device__ __forceinline__ bool wait_geq(const unsigned int* p, unsigned int target, unsigned long long limit,
-                                         Ctl* ctl, unsigned int where) {
+                                         Ctl* ctl, unsigned int where, unsigned long long& spins) {
   unsigned long long it = 0;
   while (ld_acquire(p) < target) {
     if (ld_acquire(&ctl->abort)) return false;
@@ -489,23 +612,25 @@ __device__ __forceinline__ bool wait_geq(const unsigned int* p, unsigned int tar
       atomicExch(&ctl->abort, 1u);
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(32);
   }
+  spins += it;
   return true;
 }
 
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
-          const float2* __restrict__ twg, float2* __restrict__ scratch, int nslot, int nwt, Ctl* ctl,
-          unsigned long long spin_limit) {
+          const float2* __restrict__ twg, float2* __restrict__ scratch, int nwt, Ctl* ctl, PersistParams pp) {
   extern __shared__ float2 sm[];
   __shared__ int s_t[2];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int n1 = M / kWarps, n2 = M / kWarps, n3 = (g.S + kWarps - 1) / kWarps;
   const int round = n1 + n2 + n3;
-  const long long total = (long long)(nwt + 2 * kLag) * round;
+  const int lag = pp.lag, nslot = pp.nslot;
+  const long long total = (long long)(nwt + 2 * lag) * round;
   const size_t slot_elems = wt_elems<M, OP>(g.S);
+  unsigned long long spins = 0;
   float2* tw = sm;
   float2* buf = sm + M;
   load_twiddles(tw, twg, M);
@@ -513,37 +638,36 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
   __syncthreads();
   int cur = s_t[0];
   while (cur < total) {
-    // prefetch the next ticket while this unit runs
     unsigned int nxt = 0;
-    if (threadIdx.x == 0) nxt = atomicAdd(&ctl->ticket, 1u);
+    if (threadIdx.x == 0 && pp.prefetch) nxt = atomicAdd(&ctl->ticket, 1u);
     const int r = cur / round, u = cur - (cur / round) * round;
     int phase, w, unit;
     if (u < n1) { phase = 1; w = r; unit = u; }
-    else if (u < n1 + n2) { phase = 2; w = r - kLag; unit = u - n1; }
-    else { phase = 3; w = r - 2 * kLag; unit = u - n1 - n2; }
+    else if (u < n1 + n2) { phase = 2; w = r - lag; unit = u - n1; }
+    else { phase = 3; w = r - 2 * lag; unit = u - n1 - n2; }
     const bool live = (w >= 0 && w < nwt);
     const int slot = live ? w % nslot : 0;
     const unsigned int gen = live ? (unsigned int)(w / nslot) : 0u;
     if (threadIdx.x == 0) {
       bool ok = ld_acquire(&ctl->abort) == 0u;
       if (ok && live) {
-        if (phase == 1) ok = wait_geq(&ctl->c2[slot], gen * n2, spin_limit, ctl, 1);
-        else if (phase == 2) ok = wait_geq(&ctl->c1[slot], (gen + 1) * n1, spin_limit, ctl, 2) &&
-                                  wait_geq(&ctl->c3[slot], gen * n3, spin_limit, ctl, 3);
-        else ok = wait_geq(&ctl->c2[slot], (gen + 1) * n2, spin_limit, ctl, 4);
+        if (phase == 1) ok = wait_geq(&ctl->c2[slot], gen * n2, pp.spin_limit, ctl, 1, spins);
+        else if (phase == 2) ok = wait_geq(&ctl->c1[slot], (gen + 1) * n1, pp.spin_limit, ctl, 2, spins) &&
+                                  wait_geq(&ctl->c3[slot], gen * n3, pp.spin_limit, ctl, 3, spins);
+        else ok = wait_geq(&ctl->c2[slot], (gen + 1) * n2, pp.spin_limit, ctl, 4, spins);
       }
       s_t[1] = ok ? 1 : 0;
     }
     __syncthreads();
-    if (!s_t[1]) return;
+    if (!s_t[1]) break;
     if (live) {
       float2* base = scratch + (size_t)slot * slot_elems;
       if (phase == 1) {
-        phase1<M, OP, T>(a, g, w, unit, base, buf + warp * fft_row_words(M), tw, warp, lane);
+        phase1<M, OP, T>(a, g, w, unit, base, buf + warp * row_stride<M>(), tw, warp, lane);
       } else if (phase == 2) {
         phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * kWarps, buf, tw, warp, lane);
       } else {
-        phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf + warp * fft_row_words(M), tw, warp, lane);
+        phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf, tw, warp, lane);
       }
     }
     __syncthreads();  // every thread's scratch stores of this unit are issued
@@ -552,17 +676,19 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
         __threadfence();
         atomicAdd(phase == 1 ? &ctl->c1[slot] : phase == 2 ? &ctl->c2[slot] : &ctl->c3[slot], 1u);
       }
-      s_t[0] = (int)nxt;
+      s_t[0] = pp.prefetch ? (int)nxt : (int)atomicAdd(&ctl->ticket, 1u);
     }
     __syncthreads();
     cur = s_t[0];
   }
+  if (threadIdx.x == 0 && spins) atomicAdd(&ctl->spins, spins);
 }
 
 // Bounded-wait self test: thread 0 of one CTA waits for a counter that
 // nothing increments; the wait must give up and raise the abort flag.
 __global__ void k_wait_selftest(Ctl* ctl, unsigned long long spin_limit) {
-  if (threadIdx.x == 0) wait_geq(&ctl->c1[0], 1u, spin_limit, ctl, 99);
+  unsigned long long spins = 0;
+  if (threadIdx.x == 0) wait_geq(&ctl->c1[0], 1u, spin_limit, ctl, 99, spins);
 }
 
 // dL/df = D_x^T(wx) + D_y^T(wy) on N x N, with wx, wy given on the W x W

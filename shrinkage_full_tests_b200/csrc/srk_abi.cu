@@ -79,8 +79,10 @@ struct srk_plan_s {
   unsigned int* mailbox = nullptr;     // pinned host copy of (abort, where)
   cudaEvent_t mailbox_ev = nullptr;
   bool mailbox_pending = false;
-  unsigned long long spin_limit = 1ull << 24;
-  int last_grid = 0, last_launches = 0;
+  unsigned long long spin_limit = 1ull << 25;
+  unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
+  int persist_lag = 0, persist_grid = 0, persist_prefetch = 1;
+  int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
 };
 
 namespace {
@@ -117,8 +119,9 @@ Geom adj_geom(const srk_plan_s* p, int B) {
 }
 
 size_t wt_bytes(int M, int S) {
-  const size_t fwd = (size_t)M * M + 2 * (size_t)S * M;
-  const size_t adj = 2 * (size_t)M * M + (size_t)S * M;
+  const size_t P = (size_t)s2_pitch(S);
+  const size_t fwd = (size_t)M * M + 2 * P * M;
+  const size_t adj = 2 * (size_t)M * M + P * M;
   return sizeof(float2) * (fwd > adj ? fwd : adj);
 }
 
@@ -134,30 +137,50 @@ template <int M, int OP, typename T>
 srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, bool conjG, cudaStream_t s) {
   constexpr int K = OpTraits<OP>::K;
   constexpr int L = OpTraits<OP>::L;
-  const size_t sm1 = p1_smem_bytes<M>();
-  const size_t sm2 = p2_smem_bytes(M, K, L, g.S);
-  const size_t sm3 = p3_smem_bytes<M>();
+  const size_t sm1 = phase_smem_bytes<M>();
+  const size_t sm2 = sm1;
+  const size_t sm3 = sm1;
   const size_t per = wt_elems<M, OP>(g.S);
   const size_t cap = p->scratch_bytes / sizeof(float2) / per;  // WTs that fit the scratch
   if (p->schedule == SRK_SCHEDULE_PERSISTENT && cap >= 3) {
-    const int nslot = (int)std::min<size_t>({cap, (size_t)kMaxSlots, (size_t)(2 * kLag + 2)});
     SRK_TRY(set_smem(k_persist<M, OP, T>, sm2));
     int dev = 0, nsm = 0, per_sm = 0;
     SRK_CUDA(cudaGetDevice(&dev));
     SRK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     SRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<M, OP, T>, kThreads, sm2));
     if (per_sm < 1) return fail(SRK_ERR_UNSUPPORTED, "persistent kernel does not fit an SM (smem %zu)", sm2);
-    const long long tickets = (long long)(nwt + 2 * kLag) * (M / kWarps * 2 + (g.S + kWarps - 1) / kWarps);
-    const int grid = (int)std::min<long long>((long long)nsm * per_sm, tickets);
+    const int round = M / kWarps * 2 + (g.S + kWarps - 1) / kWarps;
+    int grid = nsm * per_sm;
+    if (p->persist_grid > 0) grid = std::min(grid, p->persist_grid);
+    // Tickets in flight ~ grid (x2 with prefetch): the lag between the phases
+    // of a WT must exceed that window so a unit rarely finds its
+    // dependency unmet; the ring must hold 2*lag+2 WTs for the same reason.
+    const int window = grid * (p->persist_prefetch ? 2 : 1);
+    PersistParams pp;
+    pp.lag = p->persist_lag > 0 ? p->persist_lag : (window + round - 1) / round + 1;
+    pp.nslot = 2 * pp.lag + 2;
+    pp.prefetch = p->persist_prefetch;
+    pp.pad = 0;
+    pp.spin_limit = p->spin_limit;
+    if (pp.nslot > (int)std::min<size_t>(cap, kMaxSlots)) {
+      pp.nslot = (int)std::min<size_t>(cap, kMaxSlots);
+      pp.lag = std::min(pp.lag, pp.nslot - 1);
+    }
+    const long long tickets = (long long)(nwt + 2 * pp.lag) * round;
+    grid = (int)std::min<long long>(grid, tickets);
     SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
-    k_persist<M, OP, T><<<grid, kThreads, sm2, s>>>(a, g, p->G[0], p->G[1], conjG ? 1 : 0, p->tw, p->scratch, nslot,
-                                                   nwt, p->ctl, p->spin_limit);
+    k_persist<M, OP, T><<<grid, kThreads, sm2, s>>>(a, g, p->G[0], p->G[1], conjG ? 1 : 0, p->tw, p->scratch, nwt,
+                                                   p->ctl, pp);
     SRK_CUDA(cudaGetLastError());
     SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SRK_CUDA(cudaMemcpyAsync(p->mailbox_spins, &p->ctl->spins, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s));
     SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
     p->mailbox_pending = true;
     p->last_grid = grid;
     p->last_launches = 1;
+    p->last_lag = pp.lag;
+    p->last_nslot = pp.nslot;
     return SRK_OK;
   }
   SRK_TRY(set_smem(k_p1<M, OP, T>, sm1));
@@ -413,6 +436,10 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
       cudaSuccess)
     return cleanup(cuda_status(err, "mailbox allocation"));
   p->mailbox[0] = p->mailbox[1] = 0;
+  if ((err = cudaHostAlloc(reinterpret_cast<void**>(&p->mailbox_spins), sizeof(unsigned long long),
+                           cudaHostAllocDefault)) != cudaSuccess)
+    return cleanup(cuda_status(err, "mailbox allocation"));
+  *p->mailbox_spins = 0;
   if ((err = cudaEventCreateWithFlags(&p->mailbox_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup(cuda_status(err, "event creation"));
   std::vector<float2> tw(M);
@@ -435,6 +462,7 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->wbuf) cudaFree(p->wbuf);
   if (p->ctl) cudaFree(p->ctl);
   if (p->mailbox) cudaFreeHost(p->mailbox);
+  if (p->mailbox_spins) cudaFreeHost(p->mailbox_spins);
   if (p->mailbox_ev) cudaEventDestroy(p->mailbox_ev);
   delete p;
   return SRK_OK;
@@ -446,6 +474,8 @@ srk_status srk_plan_get_info(srk_plan p, srk_plan_info* info) {
   info->dx = p->dx; info->tile_M = p->M; info->tile_stride = p->S; info->tiles = p->T; info->tiles_adj = p->Ta;
   info->chunk_wt = p->chunk; info->scratch_bytes = p->scratch_bytes; info->dtype = p->dtype;
   info->schedule = p->schedule; info->last_launches = p->last_launches; info->last_grid = p->last_grid;
+  info->last_lag = p->last_lag; info->last_nslot = p->last_nslot;
+  info->last_spins = p->mailbox_spins ? *p->mailbox_spins : 0;
   return SRK_OK;
 }
 
@@ -454,6 +484,16 @@ srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
   if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS)
     return fail(SRK_ERR_INVALID_ARG, "bad schedule %d", (int)sch);
   p->schedule = sch;
+  return SRK_OK;
+}
+
+srk_status srk_plan_set_persistent(srk_plan p, int lag, int grid, int prefetch) {
+  if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
+  if (lag < 0 || lag > kMaxSlots / 2 - 1 || grid < 0 || (prefetch != 0 && prefetch != 1))
+    return fail(SRK_ERR_INVALID_ARG, "bad persistent parameters lag=%d grid=%d prefetch=%d", lag, grid, prefetch);
+  p->persist_lag = lag;
+  p->persist_grid = grid;
+  p->persist_prefetch = prefetch;
   return SRK_OK;
 }
 
