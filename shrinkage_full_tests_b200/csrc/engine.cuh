@@ -221,7 +221,7 @@ __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int 
 // loads need no test; erosion 0 takes the tested path.
 template <typename T>
 struct GradCol {
-  const T* c;   // f + gx*N + gy0
+  const T* __restrict__ c;   // f + gx*N + gy0
   int N;
   bool tested;
   int gx, gy0;
@@ -251,56 +251,74 @@ __device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int
   return gc;
 }
 
-// ---- epilogues: P3 hands over column x (local, valid) of work tile w ------
-// zx = IFFT(Z*Gx), zy = IFFT(Z*Gy) (OP != ADJ), or z = IFFT(sum) (ADJ).
+// Rows of this lane that carry valid outputs, as a bit mask over i.
+template <int M>
+__device__ __forceinline__ unsigned valid_rows(const Geom& g, int y0, int lane) {
+  unsigned m = 0;
+#pragma unroll
+  for (int i = 0; i < M / 32; ++i) {
+    const int y = lane + 32 * i;
+    if (y >= g.e && y < g.e + g.S && y0 + y - g.e < g.Wout) m |= 1u << i;
+  }
+  return m;
+}
+
 template <int M, int OP, typename T>
 __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, int w, int x, int lane,
-                                                const float2 (&z0)[M / 32], const float2 (&z1)[M / 32]) {
+                                                float2 (&z0)[M / 32], float2 (&z1)[M / 32]) {
   constexpr int EPT = M / 32;
   const int N = a.N, W = a.W, e = a.e;
-  // rows handled by this lane: y = lane + 32 i valid iff y in [e, e+S) and
-  // its output row y0 + y - e < Wout
-  auto valid_row = [&](const TileRef& t, int i) {
-    const int y = lane + 32 * i;
-    return y >= g.e && y < g.e + g.S && t.y0 + y - g.e < g.Wout;
-  };
   if constexpr (OP == OP_FWD || OP == OP_VJP_F) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const TileRef t = tile_of(g, 2 * w + h);
       const int ox = t.x0 + x - g.e;
       if (!t.live || ox >= g.Wout) continue;
-      // output row oy = y0 + y - e  ->  pointer to row (y0 - e + lane)
+      const unsigned vm = valid_rows<M>(g, t.y0, lane);
+      // output row oy = y0 + y - e  ->  offset of row (y0 - e + lane)
       const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
       if constexpr (OP == OP_FWD) {
-        const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e,
-                                       t.y0 + lane);
-        T* R = static_cast<T*>(a.out0);
-        T* UX = static_cast<T*>(a.out_ux);
-        T* UY = static_cast<T*>(a.out_uy);
+        T* __restrict__ R = static_cast<T*>(a.out0);
+        T* __restrict__ UX = static_cast<T*>(a.out_ux);
+        T* __restrict__ UY = static_cast<T*>(a.out_uy);
+        if (UX) {
 #pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-          if (!valid_row(t, i)) continue;
-          const float ux = h ? z0[i].y : z0[i].x;
-          const float uy = h ? z1[i].y : z1[i].x;
-          if (R) {
-            float fx, fy;
-            gc.at(i, fx, fy);
-            stf(R, ob + 32 * i, ux * fx + uy * fy);
+          for (int i = 0; i < EPT; ++i)
+            if (vm >> i & 1u) stf(UX, ob + 32 * i, h ? z0[i].y : z0[i].x);
+        }
+        if (UY) {
+#pragma unroll
+          for (int i = 0; i < EPT; ++i)
+            if (vm >> i & 1u) stf(UY, ob + 32 * i, h ? z1[i].y : z1[i].x);
+        }
+        if (R) {
+          const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e,
+                                         t.y0 + lane);
+          // gradients for all rows first (every load in flight before the
+          // first store); the result overwrites this image's half of z0
+#pragma unroll
+          for (int i = 0; i < EPT; ++i) {
+            float fx = 0.f, fy = 0.f;
+            if (vm >> i & 1u) gc.at(i, fx, fy);
+            float& o = h ? z0[i].y : z0[i].x;
+            o = o * fx + (h ? z1[i].y : z1[i].x) * fy;
           }
-          if (UX) stf(UX, ob + 32 * i, ux);
-          if (UY) stf(UY, ob + 32 * i, uy);
+#pragma unroll
+          for (int i = 0; i < EPT; ++i)
+            if (vm >> i & 1u) stf(R, ob + 32 * i, h ? z0[i].y : z0[i].x);
         }
       } else {  // OP_VJP_F: w = u * v
-        const T* V = static_cast<const T*>(a.v);
-        float* WX = static_cast<float*>(a.out0);
-        float* WY = static_cast<float*>(a.out1);
+        const T* __restrict__ V = static_cast<const T*>(a.v);
+        float* __restrict__ WX = static_cast<float*>(a.out0);
+        float* __restrict__ WY = static_cast<float*>(a.out1);
+        float v[EPT];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) v[i] = (vm >> i & 1u) ? ldf(V, ob + 32 * i) : 0.f;
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
-          if (!valid_row(t, i)) continue;
-          const float v = ldf(V, ob + 32 * i);
-          WX[ob + 32 * i] = (h ? z0[i].y : z0[i].x) * v;
-          WY[ob + 32 * i] = (h ? z1[i].y : z1[i].x) * v;
+          if (!(vm >> i & 1u)) continue;
+          WX[ob + 32 * i] = (h ? z0[i].y : z0[i].x) * v[i];
+          WY[ob + 32 * i] = (h ? z1[i].y : z1[i].x) * v[i];
         }
       }
     }
@@ -308,28 +326,36 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
     const TileRef t = tile_of(g, w);
     const int ox = t.x0 + x - g.e;
     if (ox >= g.Wout) return;
+    const unsigned vm = valid_rows<M>(g, t.y0, lane);
     const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
     if constexpr (OP == OP_JVP) {
       // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52); re: conv of g, im: conv of dg
       const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
       const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
+      T* __restrict__ DH = static_cast<T*>(a.out0);
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
-        if (!valid_row(t, i)) continue;
-        float fx, fy, dfx, dfy;
-        gf.at(i, fx, fy);
-        gd.at(i, dfx, dfy);
-        stf(static_cast<T*>(a.out0), ob + 32 * i, z0[i].y * fx + z1[i].y * fy + z0[i].x * dfx + z1[i].x * dfy);
+        float fx = 0.f, fy = 0.f, dfx = 0.f, dfy = 0.f;
+        if (vm >> i & 1u) {
+          gf.at(i, fx, fy);
+          gd.at(i, dfx, dfy);
+        }
+        z0[i].x = z0[i].y * fx + z1[i].y * fy + z0[i].x * dfx + z1[i].x * dfy;
       }
+#pragma unroll
+      for (int i = 0; i < EPT; ++i)
+        if (vm >> i & 1u) stf(DH, ob + 32 * i, z0[i].x);
     } else {
-      const T* LAM = static_cast<const T*>(a.v);
-      const T* DLAM = static_cast<const T*>(a.dv);
+      const T* __restrict__ LAM = static_cast<const T*>(a.v);
+      const T* __restrict__ DLAM = static_cast<const T*>(a.dv);
+      float* __restrict__ WX = static_cast<float*>(a.out0);
+      float* __restrict__ WY = static_cast<float*>(a.out1);
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
-        if (!valid_row(t, i)) continue;
+        if (!(vm >> i & 1u)) continue;
         const float lam = ldf(LAM, ob + 32 * i), dlam = ldf(DLAM, ob + 32 * i);
-        static_cast<float*>(a.out0)[ob + 32 * i] = dlam * z0[i].x + lam * z0[i].y;
-        static_cast<float*>(a.out1)[ob + 32 * i] = dlam * z1[i].x + lam * z1[i].y;
+        WX[ob + 32 * i] = dlam * z0[i].x + lam * z0[i].y;
+        WY[ob + 32 * i] = dlam * z1[i].x + lam * z1[i].y;
       }
     }
   } else {  // OP_ADJ: output is the full N x N image
@@ -338,12 +364,12 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
       const TileRef t = tile_of(g, 2 * w + h);
       const int ox = t.x0 + x - g.e;
       if (!t.live || ox >= g.Wout) continue;
+      const unsigned vm = valid_rows<M>(g, t.y0, lane);
       const long long ob = (long long)t.b * N * N + (long long)ox * N + t.y0 - g.e + lane;
+      T* __restrict__ O = static_cast<T*>(a.out0);
 #pragma unroll
-      for (int i = 0; i < EPT; ++i) {
-        if (!valid_row(t, i)) continue;
-        stf(static_cast<T*>(a.out0), ob + 32 * i, h ? z0[i].y : z0[i].x);
-      }
+      for (int i = 0; i < EPT; ++i)
+        if (vm >> i & 1u) stf(O, ob + 32 * i, h ? z0[i].y : z0[i].x);
     }
   }
 }
@@ -407,19 +433,27 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
   }
 }
 
-// Transposing copy: 8 consecutive columns [c0, c0+8) of a column-contiguous
-// block (column pitch `pitch`, M rows) into 8 staging rows, one per column.
-// Columns >= ncol are not read.  All threads of the CTA take part.
+// Transposing copy of an M x 8 block (M lines of 8 consecutive complex
+// values, line pitch `pitch`) into 8 staging rows of M values each.  All
+// threads of the CTA take part.
 template <int M>
-__device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int pitch, int ncol,
-                                           float2* __restrict__ rows) {
+__device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int pitch, float2* __restrict__ rows) {
   constexpr int RS = row_stride<M>();
-  for (int idx = threadIdx.x; idx < M * 4; idx += kThreads) {
+  constexpr int NIT = M * 4 / kThreads;  // float4 loads per thread
+  static_assert(M * 4 % kThreads == 0, "staging loop must divide evenly");
+  // all loads in flight first, then the scattered shared stores
+  float4 q[NIT];
+#pragma unroll
+  for (int j = 0; j < NIT; ++j) {
+    const int idx = threadIdx.x + j * kThreads;
+    q[j] = __ldcg(reinterpret_cast<const float4*>(src + (size_t)(idx >> 2) * pitch + 2 * (idx & 3)));
+  }
+#pragma unroll
+  for (int j = 0; j < NIT; ++j) {
+    const int idx = threadIdx.x + j * kThreads;
     const int y = idx >> 2, cp = idx & 3;
-    if (2 * cp >= ncol) continue;
-    const float4 q = __ldcg(reinterpret_cast<const float4*>(src + (size_t)y * pitch + 2 * cp));
-    rows[(2 * cp) * RS + fft_pad(y)] = make_float2(q.x, q.y);
-    rows[(2 * cp + 1) * RS + fft_pad(y)] = make_float2(q.z, q.w);
+    rows[(2 * cp) * RS + fft_pad(y)] = make_float2(q[j].x, q[j].y);
+    rows[(2 * cp + 1) * RS + fft_pad(y)] = make_float2(q[j].z, q[j].w);
   }
 }
 
@@ -436,16 +470,8 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
   const int S = g.S, e = g.e, P = s2_pitch(S);
   // S1 viewed as rows ky (pitch M) of columns x: a transposing copy of the
   // 8 columns ky0.. of the (x, ky) matrix -- i.e. S1[k][x][ky0 + c].
-  for (int k = 0; k < K; ++k) {
-    const float2* src = S1 + (size_t)k * M * M + ky0;
-    float2* dst = rows + k * kWarps * RS;
-    for (int idx = threadIdx.x; idx < M * 4; idx += kThreads) {
-      const int x = idx >> 2, rp = idx & 3;
-      const float4 q = __ldcg(reinterpret_cast<const float4*>(src + (size_t)x * M + 2 * rp));
-      dst[(2 * rp) * RS + fft_pad(x)] = make_float2(q.x, q.y);
-      dst[(2 * rp + 1) * RS + fft_pad(x)] = make_float2(q.z, q.w);
-    }
-  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) stage_rows<M>(S1 + (size_t)k * M * M + ky0, M, rows + k * kWarps * RS);
   __syncthreads();
   const int ky = ky0 + warp;
   float2* row0 = rows + warp * RS;              // field 0 / exchange
@@ -500,8 +526,8 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   constexpr int RS = row_stride<M>();
   const int P = s2_pitch(g.S);
   const int x0 = xb * kWarps;
-  for (int l = 0; l < L; ++l)
-    stage_rows<M>(S2 + (size_t)l * M * P + x0, P, P - x0, rows + l * kWarps * RS);
+#pragma unroll
+  for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * kWarps * RS);
   __syncthreads();
   const int xv = x0 + warp;
   if (xv >= g.S) return;
