@@ -89,11 +89,19 @@ const char* srk_last_error(void);
  * B_max: largest batch a call may pass.
  * spectra_M: FFT size of the caller's spectra (N for srkTrainingForward,
  *            the reference's M_TILE for the OaS operators).
- * tile_M: 0 = choose automatically, else 128, 256 or 512.
+ * tile_M: 0 = choose by a cost model, SRK_TILE_AUTOTUNE = time every
+ *         (tile, schedule) candidate once per device and configuration
+ *         (cached on disk, see srk_autotune), else 128, 256 or 512.
  * scratch_budget_bytes: 0 = default (1 GiB). */
 srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, int B_max, int spectra_M,
                            srk_dtype dtype, int tile_M, size_t scratch_budget_bytes);
 srk_status srk_plan_destroy(srk_plan plan);
+#define SRK_TILE_AUTOTUNE (-1)
+/* Time every (tile size, schedule) candidate of the forward operator for this
+ * configuration on synthetic device data (up to 512 images) and return the
+ * fastest.  Results are cached per device name and configuration in the file
+ * named by $SRK_TUNE_CACHE (default ~/.cache/srk_b200_tune.txt). */
+srk_status srk_autotune(int N, int W, int erosion, float dx, int B, srk_dtype dtype, int* tile_M, int* schedule);
 srk_status srk_plan_get_info(srk_plan plan, srk_plan_info* info);
 srk_status srk_plan_set_adj_convention(srk_plan plan, srk_adj_convention conv);
 srk_status srk_plan_set_schedule(srk_plan plan, srk_schedule schedule);
@@ -179,6 +187,35 @@ srk_status srk_vjp(const float* d_v, const float* d_f, const float* d_g, int B, 
                    float* d_dLdf, float* d_dLdg, srk_plan plan);
 srk_status srk_jvp(const float* d_f, const float* d_g, const float* d_df, const float* d_dg, int B,
                    srk_stream_t stream, float* d_dh, srk_plan plan);
+
+/* ---- storage-typed forms ----------------------------------------------------
+ * Same operators with every image / cotangent / output buffer in the plan's
+ * storage type (SRK_F32: float, SRK_F16: IEEE half, SRK_BF16: bfloat16),
+ * passed as void*.  Arithmetic is FP32 throughout (every butterfly, the
+ * spectral products and the combine); kernel spectra and the intermediate
+ * spectra stay FP32.  The float* entry points above require an SRK_F32 plan.
+ * No counterpart in the reference (its operators are fp32 only). */
+srk_status srk_training_forward_t(const void* d_E, const void* d_I, const void* d_Gx_freq, const void* d_Gy_freq,
+                                  int N, int W, int erosion, float dx, int B, srk_stream_t stream, void* d_R,
+                                  srk_plan plan);
+srk_status srk_forward_oas_t(const void* d_E, const void* d_I, const void* d_Gx_freq, const void* d_Gy_freq, int N,
+                             int W, int erosion, float dx, srk_stream_t stream, void* d_R, srk_plan plan, void* d_ux,
+                             void* d_uy);
+srk_status srk_adjoint_t(const void* d_v, const void* d_ux, const void* d_uy, const void* d_I, const void* d_Gx_freq,
+                         const void* d_Gy_freq, int N, int W, int erosion, float dx, srk_stream_t stream,
+                         void* d_dLdI, void* d_dLdE, srk_plan plan);
+srk_status srk_tangent_t(const void* d_f, const void* d_g, const void* d_df, const void* d_dg, const void* d_Gx_freq,
+                         const void* d_Gy_freq, int N, int W, int erosion, float dx, srk_stream_t stream, void* d_dh,
+                         srk_plan plan);
+srk_status srk_tangent_adjoint_t(const void* d_f, const void* d_g, const void* d_df, const void* d_dg,
+                                 const void* d_lam_h, const void* d_dlam_h, const void* d_Gx_freq,
+                                 const void* d_Gy_freq, int N, int W, int erosion, float dx, srk_stream_t stream,
+                                 void* d_dLam_f, void* d_dLam_g, srk_plan plan);
+srk_status srk_forward_t(const void* d_f, const void* d_g, int B, srk_stream_t stream, void* d_h, srk_plan plan);
+srk_status srk_vjp_t(const void* d_v, const void* d_f, const void* d_g, int B, srk_stream_t stream, void* d_dLdf,
+                     void* d_dLdg, srk_plan plan);
+srk_status srk_jvp_t(const void* d_f, const void* d_g, const void* d_df, const void* d_dg, int B,
+                     srk_stream_t stream, void* d_dh, srk_plan plan);
 
 #ifdef __cplusplus
 }

@@ -66,6 +66,7 @@ _SIGS = {
     "srk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "srk_plan_set_adj_convention": [_P, _I],
     "srk_plan_set_schedule": [_P, _I],
+    "srk_autotune": [_I, _I, _I, _F, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "srk_plan_set_persistent": [_P, _I, _I, _I],
     "srk_plan_sync": [_P, _P],
     "srk_debug_wait_selftest": [_P, ctypes.c_ulonglong, _P],
@@ -83,6 +84,10 @@ _SIGS = {
     "srk_vjp": [_P, _P, _P, _I, _P, _P, _P, _P],
     "srk_jvp": [_P, _P, _P, _P, _I, _P, _P, _P],
 }
+# storage-typed forms (void* buffers in the plan's dtype): same argument types
+for _n in ("srk_training_forward", "srk_forward_oas", "srk_adjoint", "srk_tangent", "srk_tangent_adjoint",
+           "srk_forward", "srk_vjp", "srk_jvp"):
+    _SIGS[_n + "_t"] = _SIGS[_n]
 _RESTYPE = {"srk_version": _I, "srk_status_string": ctypes.c_char_p, "srk_last_error": ctypes.c_char_p}
 
 
@@ -140,6 +145,7 @@ class SrkPlan:
                                      spectra_M if spectra_M is not None else N, dtype, tile_M, scratch_budget))
         self.handle = h.value
         self.N, self.W, self.erosion, self.dx, self.B_max = N, W, erosion, dx, B_max
+        self.dtype = dtype
 
     def info(self):
         i = PlanInfo()
@@ -182,31 +188,48 @@ class SrkPlan:
             pass
 
 
+SRK_TILE_AUTOTUNE = -1
+
+
+def autotune(N, W, erosion, dx=1.0, B=1, dtype=SRK_F32):
+    """(tile_M, schedule) the library picks for this configuration (timed once
+    per device, then cached on disk)."""
+    m, sc = _I(), _I()
+    _check(lib().srk_autotune(N, W, erosion, dx, B, dtype, ctypes.byref(m), ctypes.byref(sc)))
+    return m.value, sc.value
+
+
+def _entry(name, ws):
+    """fp32 plans use the reference-typed (float*) entry point, fp16/bf16
+    plans the storage-typed _t form."""
+    return getattr(lib(), name if ws.dtype == SRK_F32 else name + "_t")
+
+
 def srkTrainingForward(E, I, Gx_freq, Gy_freq, N, W, erosion, dx, B, stream, R, ws):
-    _check(lib().srk_training_forward(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, B,
-                                      _stream(stream), _ptr(R), ws.handle))
+    _check(_entry("srk_training_forward", ws)(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, B,
+                                              _stream(stream), _ptr(R), ws.handle))
 
 
 def srkForwardOaS(E, I, Gx_freq, Gy_freq, N, W, erosion, dx, stream, R, ws, ux=None, uy=None):
-    _check(lib().srk_forward_oas(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx,
-                                 _stream(stream), _ptr(R), ws.handle, _ptr(ux), _ptr(uy)))
+    _check(_entry("srk_forward_oas", ws)(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx,
+                                         _stream(stream), _ptr(R), ws.handle, _ptr(ux), _ptr(uy)))
 
 
 def adjointSRK(v, ux, uy, I, Gx_freq, Gy_freq, N, W, erosion, dx, stream, dLdI, dLdE, ws):
-    _check(lib().srk_adjoint(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion,
-                             dx, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
+    _check(_entry("srk_adjoint", ws)(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, W,
+                                     erosion, dx, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
 
 
 def shrinkageTangentOaS(f, g, df, dg, Gx_freq, Gy_freq, N, W, erosion, dx, stream, dh, ws):
-    _check(lib().srk_tangent(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion,
-                             dx, _stream(stream), _ptr(dh), ws.handle))
+    _check(_entry("srk_tangent", ws)(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(Gx_freq), _ptr(Gy_freq), N, W,
+                                     erosion, dx, _stream(stream), _ptr(dh), ws.handle))
 
 
 def shrinkageTangentAdjointOaS(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_freq, N, W, erosion, dx, stream,
                                dLam_f, dLam_g, ws):
-    _check(lib().srk_tangent_adjoint(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
-                                     _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, _stream(stream),
-                                     _ptr(dLam_f), _ptr(dLam_g), ws.handle))
+    _check(_entry("srk_tangent_adjoint", ws)(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
+                                             _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, _stream(stream),
+                                             _ptr(dLam_f), _ptr(dLam_g), ws.handle))
 
 
 def srkPrecomputeKernelFreq(K, kw, kh, M, G_freq, stream=None):
@@ -222,12 +245,12 @@ def green_tensor(Kx, Ky, gamma, R_w, dx, stream=None):
 
 
 def forward(f, g, B, h, ws, stream=None):
-    _check(lib().srk_forward(_ptr(f), _ptr(g), B, _stream(stream), _ptr(h), ws.handle))
+    _check(_entry("srk_forward", ws)(_ptr(f), _ptr(g), B, _stream(stream), _ptr(h), ws.handle))
 
 
 def vjp(v, f, g, B, dLdf, dLdg, ws, stream=None):
-    _check(lib().srk_vjp(_ptr(v), _ptr(f), _ptr(g), B, _stream(stream), _ptr(dLdf), _ptr(dLdg), ws.handle))
+    _check(_entry("srk_vjp", ws)(_ptr(v), _ptr(f), _ptr(g), B, _stream(stream), _ptr(dLdf), _ptr(dLdg), ws.handle))
 
 
 def jvp(f, g, df, dg, B, dh, ws, stream=None):
-    _check(lib().srk_jvp(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), B, _stream(stream), _ptr(dh), ws.handle))
+    _check(_entry("srk_jvp", ws)(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), B, _stream(stream), _ptr(dh), ws.handle))

@@ -22,19 +22,36 @@ def deps():
 
 
 def build(force=False, verbose=False):
+    """Compile every .cu to an object in parallel (one kernel family per
+    storage type), then link the shared library."""
     if not force and os.path.exists(LIB):
         t = os.path.getmtime(LIB)
         if all(os.path.getmtime(s) <= t for s in deps()):
             return LIB
-    cmd = [NVCC] + FLAGS + ["-I" + os.path.join(ROOT, "include")] + sources() + ["-o", LIB + ".tmp"]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    obj_dir = os.path.join(PKG, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in FLAGS if f != "-shared"]
+    procs = []
+    for src in sources():
+        obj = os.path.join(obj_dir, os.path.basename(src)[:-3] + ".o")
+        cmd = [NVCC] + compile_flags + ["-I" + os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((cmd, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs = []
+    for cmd, obj, pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError("nvcc failed:\n%s\n%s%s" % (" ".join(cmd), out, err))
+        if verbose:
+            sys.stderr.write(err)
+        objs.append(obj)
+    link = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC"] + objs + \
+        ["-o", LIB + ".tmp"]
+    r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n%s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
+        raise RuntimeError("link failed:\n%s\n%s%s" % (" ".join(link), r.stdout, r.stderr))
     os.replace(LIB + ".tmp", LIB)
-    if verbose:
-        sys.stderr.write(r.stderr)
     return LIB
 
 

@@ -1,0 +1,100 @@
+// conv_launch.cuh — launch sequences of the engine (both schedules) for one
+// operator and storage type; included by conv_<type>.cu only.
+#pragma once
+#include "internal.h"
+
+namespace srk {
+
+template <typename K>
+srk_status set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024)
+    SRK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return SRK_OK;
+}
+
+template <int M, int OP, typename T>
+srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, bool conjG, cudaStream_t s) {
+  constexpr int K = OpTraits<OP>::K;
+  constexpr int L = OpTraits<OP>::L;
+  const size_t sm1 = phase_smem_bytes<M>();
+  const size_t sm2 = sm1;
+  const size_t sm3 = sm1;
+  const size_t per = wt_elems<M, OP>(g.S);
+  const size_t cap = p->scratch_bytes / sizeof(float2) / per;  // WTs that fit the scratch
+  if (p->schedule == SRK_SCHEDULE_PERSISTENT && cap >= 3) {
+    SRK_TRY(set_smem(k_persist<M, OP, T>, sm2));
+    int dev = 0, nsm = 0, per_sm = 0;
+    SRK_CUDA(cudaGetDevice(&dev));
+    SRK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    SRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<M, OP, T>, kThreads, sm2));
+    if (per_sm < 1) return fail(SRK_ERR_UNSUPPORTED, "persistent kernel does not fit an SM (smem %zu)", sm2);
+    const int round = M / kWarps * 2 + (g.S + kWarps - 1) / kWarps;
+    int grid = nsm * per_sm;
+    if (p->persist_grid > 0) grid = std::min(grid, p->persist_grid);
+    // Tickets in flight ~ grid (x2 with prefetch): the lag between the phases
+    // of a WT must exceed that window so a unit rarely finds its
+    // dependency unmet; the ring must hold 2*lag+2 WTs for the same reason.
+    const int window = grid * (p->persist_prefetch ? 2 : 1);
+    PersistParams pp;
+    pp.lag = p->persist_lag > 0 ? p->persist_lag : (window + round - 1) / round + 1;
+    pp.nslot = 2 * pp.lag + 2;
+    pp.prefetch = p->persist_prefetch;
+    pp.pad = 0;
+    pp.spin_limit = p->spin_limit;
+    if (pp.nslot > (int)std::min<size_t>(cap, kMaxSlots)) {
+      pp.nslot = (int)std::min<size_t>(cap, kMaxSlots);
+      pp.lag = std::min(pp.lag, pp.nslot - 1);
+    }
+    const long long tickets = (long long)(nwt + 2 * pp.lag) * round;
+    grid = (int)std::min<long long>(grid, tickets);
+    SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
+    k_persist<M, OP, T><<<grid, kThreads, sm2, s>>>(a, g, p->G[0], p->G[1], conjG ? 1 : 0, p->tw, p->scratch, nwt,
+                                                   p->ctl, pp);
+    SRK_CUDA(cudaGetLastError());
+    SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    SRK_CUDA(cudaMemcpyAsync(p->mailbox_spins, &p->ctl->spins, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s));
+    SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
+    p->mailbox_pending = true;
+    p->last_grid = grid;
+    p->last_launches = 1;
+    p->last_lag = pp.lag;
+    p->last_nslot = pp.nslot;
+    return SRK_OK;
+  }
+  SRK_TRY(set_smem(k_p1<M, OP, T>, sm1));
+  SRK_TRY(set_smem(k_p2<M, OP>, sm2));
+  SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
+  const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
+  int launches = 0;
+  for (int w0 = 0; w0 < nwt; w0 += chunk) {
+    const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
+    k_p1<M, OP, T><<<dim3(M / kWarps, c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
+    k_p2<M, OP><<<dim3(M / kWarps, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
+    k_p3<M, OP, T><<<dim3((g.S + kWarps - 1) / kWarps, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
+    launches += 3;
+  }
+  p->last_launches = launches;
+  return cuda_status(cudaGetLastError(), "conv launch");
+}
+
+template <int OP, typename T>
+srk_status launch_conv(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s) {
+  const int nwt = OpTraits<OP>::PAIRS ? (g.U + 1) / 2 : g.U;
+  if (nwt <= 0) return SRK_OK;
+  switch (p->M) {
+    case 128: return launch_conv_m<128, OP, T>(p, a, g, nwt, conjG, s);
+    case 256: return launch_conv_m<256, OP, T>(p, a, g, nwt, conjG, s);
+    case 512: return launch_conv_m<512, OP, T>(p, a, g, nwt, conjG, s);
+    default: return fail(SRK_ERR_UNSUPPORTED, "tile size %d not built", p->M);
+  }
+}
+
+}  // namespace srk
+
+#define SRK_INSTANTIATE_CONV(T)                                                                        \
+  template srk_status srk::launch_conv<srk::OP_FWD, T>(srk_plan_s*, const srk::OpArgs&, const srk::Geom&, bool, cudaStream_t);      \
+  template srk_status srk::launch_conv<srk::OP_VJP_F, T>(srk_plan_s*, const srk::OpArgs&, const srk::Geom&, bool, cudaStream_t);    \
+  template srk_status srk::launch_conv<srk::OP_JVP, T>(srk_plan_s*, const srk::OpArgs&, const srk::Geom&, bool, cudaStream_t);      \
+  template srk_status srk::launch_conv<srk::OP_TANADJ_F, T>(srk_plan_s*, const srk::OpArgs&, const srk::Geom&, bool, cudaStream_t); \
+  template srk_status srk::launch_conv<srk::OP_ADJ, T>(srk_plan_s*, const srk::OpArgs&, const srk::Geom&, bool, cudaStream_t);

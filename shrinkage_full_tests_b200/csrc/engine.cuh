@@ -712,7 +712,7 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
 
 // Bounded-wait self test: thread 0 of one CTA waits for a counter that
 // nothing increments; the wait must give up and raise the abort flag.
-__global__ void k_wait_selftest(Ctl* ctl, unsigned long long spin_limit) {
+static __global__ void k_wait_selftest(Ctl* ctl, unsigned long long spin_limit) {
   unsigned long long spins = 0;
   if (threadIdx.x == 0) wait_geq(&ctl->c1[0], 1u, spin_limit, ctl, 99, spins);
 }

@@ -1,0 +1,81 @@
+// internal.h — private declarations shared by the library's translation
+// units: status helpers, the plan object, and the engine launchers (one
+// explicit instantiation per storage type lives in conv_<type>.cu so the
+// kernel families compile in parallel).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/srk_b200.h"
+#include "engine.cuh"
+
+namespace srk {
+
+inline thread_local std::string g_last_error;
+
+inline srk_status fail(srk_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+inline srk_status cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SRK_OK;
+  return fail(e == cudaErrorMemoryAllocation ? SRK_ERR_ALLOC : SRK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define SRK_TRY(expr)                        \
+  do {                                       \
+    const srk_status _s = (expr);            \
+    if (_s != SRK_OK) return _s;             \
+  } while (0)
+#define SRK_CUDA(expr) SRK_TRY(cuda_status((expr), #expr))
+
+}  // namespace srk
+
+struct srk_plan_s {
+  int device = 0;
+  int N = 0, W = 0, e = 0, B_max = 0, spectra_M = 0;
+  float dx = 1.f;
+  srk_dtype dtype = SRK_F32;
+  srk_adj_convention conv = SRK_ADJ_REFERENCE;
+  int M = 0, S = 0, T = 0, Ta = 0;
+  int chunk = 0;
+  float2* G[2] = {nullptr, nullptr};   // engine-layout spectra, scaled by dx^2/M^2
+  bool have_G = false;
+  const void* src[2] = {nullptr, nullptr};
+  float2* tw = nullptr;                // W_M^m, float
+  float2* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  float* wbuf = nullptr;               // wx, wy for dL/df
+  size_t wbuf_bytes = 0;
+  int schedule = SRK_SCHEDULE_THREE_PASS;
+  srk::Ctl* ctl = nullptr;             // persistent-kernel control block
+  unsigned int* mailbox = nullptr;     // pinned host copy of (abort, where)
+  cudaEvent_t mailbox_ev = nullptr;
+  bool mailbox_pending = false;
+  unsigned long long spin_limit = 1ull << 25;
+  unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
+  int persist_lag = 0, persist_grid = 0, persist_prefetch = 1;
+  int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
+};
+
+namespace srk {
+
+// Run one engine operator over all work tiles of geometry g (conv_<type>.cu).
+template <int OP, typename T>
+srk_status launch_conv(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s);
+
+}  // namespace srk

@@ -9,42 +9,17 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
+#include <sys/stat.h>
 #include <string>
 #include <vector>
 
-#include "../../include/srk_b200.h"
-#include "engine.cuh"
+#include "internal.h"
 #include "spectra.cuh"
 
 using namespace srk;
 
 namespace {
-
-thread_local std::string g_last_error;
-
-srk_status fail(srk_status s, const char* fmt, ...) {
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof(buf), fmt, ap);
-  va_end(ap);
-  g_last_error = buf;
-  return s;
-}
-
-srk_status cuda_status(cudaError_t e, const char* what) {
-  if (e == cudaSuccess) return SRK_OK;
-  return fail(e == cudaErrorMemoryAllocation ? SRK_ERR_ALLOC : SRK_ERR_CUDA, "%s: %s", what,
-              cudaGetErrorString(e));
-}
-
-#define SRK_TRY(expr)                        \
-  do {                                       \
-    const srk_status _s = (expr);            \
-    if (_s != SRK_OK) return _s;             \
-  } while (0)
-#define SRK_CUDA(expr) SRK_TRY(cuda_status((expr), #expr))
-
 
 // Host double-precision twiddle table (cos, sin)(2 pi m / M).
 std::vector<double2> twiddles64(int M) {
@@ -58,32 +33,7 @@ std::vector<double2> twiddles64(int M) {
 
 }  // namespace
 
-struct srk_plan_s {
-  int device = 0;
-  int N = 0, W = 0, e = 0, B_max = 0, spectra_M = 0;
-  float dx = 1.f;
-  srk_dtype dtype = SRK_F32;
-  srk_adj_convention conv = SRK_ADJ_REFERENCE;
-  int M = 0, S = 0, T = 0, Ta = 0;
-  int chunk = 0;
-  float2* G[2] = {nullptr, nullptr};   // engine-layout spectra, scaled by 1/M^2
-  bool have_G = false;
-  const void* src[2] = {nullptr, nullptr};
-  float2* tw = nullptr;                // W_M^m, float
-  float2* scratch = nullptr;
-  size_t scratch_bytes = 0;
-  float* wbuf = nullptr;               // wx, wy for dL/df
-  size_t wbuf_bytes = 0;
-  int schedule = SRK_SCHEDULE_PERSISTENT;
-  Ctl* ctl = nullptr;                  // persistent-kernel control block
-  unsigned int* mailbox = nullptr;     // pinned host copy of (abort, where)
-  cudaEvent_t mailbox_ev = nullptr;
-  bool mailbox_pending = false;
-  unsigned long long spin_limit = 1ull << 25;
-  unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
-  int persist_lag = 0, persist_grid = 0, persist_prefetch = 1;
-  int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
-};
+
 
 namespace {
 
@@ -126,89 +76,15 @@ size_t wt_bytes(int M, int S) {
 }
 
 // ---- launch helpers -------------------------------------------------------------
-template <typename K>
-srk_status set_smem(K kernel, size_t bytes) {
-  if (bytes > 48 * 1024)
-    SRK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  return SRK_OK;
-}
-
-template <int M, int OP, typename T>
-srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, bool conjG, cudaStream_t s) {
-  constexpr int K = OpTraits<OP>::K;
-  constexpr int L = OpTraits<OP>::L;
-  const size_t sm1 = phase_smem_bytes<M>();
-  const size_t sm2 = sm1;
-  const size_t sm3 = sm1;
-  const size_t per = wt_elems<M, OP>(g.S);
-  const size_t cap = p->scratch_bytes / sizeof(float2) / per;  // WTs that fit the scratch
-  if (p->schedule == SRK_SCHEDULE_PERSISTENT && cap >= 3) {
-    SRK_TRY(set_smem(k_persist<M, OP, T>, sm2));
-    int dev = 0, nsm = 0, per_sm = 0;
-    SRK_CUDA(cudaGetDevice(&dev));
-    SRK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    SRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<M, OP, T>, kThreads, sm2));
-    if (per_sm < 1) return fail(SRK_ERR_UNSUPPORTED, "persistent kernel does not fit an SM (smem %zu)", sm2);
-    const int round = M / kWarps * 2 + (g.S + kWarps - 1) / kWarps;
-    int grid = nsm * per_sm;
-    if (p->persist_grid > 0) grid = std::min(grid, p->persist_grid);
-    // Tickets in flight ~ grid (x2 with prefetch): the lag between the phases
-    // of a WT must exceed that window so a unit rarely finds its
-    // dependency unmet; the ring must hold 2*lag+2 WTs for the same reason.
-    const int window = grid * (p->persist_prefetch ? 2 : 1);
-    PersistParams pp;
-    pp.lag = p->persist_lag > 0 ? p->persist_lag : (window + round - 1) / round + 1;
-    pp.nslot = 2 * pp.lag + 2;
-    pp.prefetch = p->persist_prefetch;
-    pp.pad = 0;
-    pp.spin_limit = p->spin_limit;
-    if (pp.nslot > (int)std::min<size_t>(cap, kMaxSlots)) {
-      pp.nslot = (int)std::min<size_t>(cap, kMaxSlots);
-      pp.lag = std::min(pp.lag, pp.nslot - 1);
-    }
-    const long long tickets = (long long)(nwt + 2 * pp.lag) * round;
-    grid = (int)std::min<long long>(grid, tickets);
-    SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
-    k_persist<M, OP, T><<<grid, kThreads, sm2, s>>>(a, g, p->G[0], p->G[1], conjG ? 1 : 0, p->tw, p->scratch, nwt,
-                                                   p->ctl, pp);
-    SRK_CUDA(cudaGetLastError());
-    SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
-    SRK_CUDA(cudaMemcpyAsync(p->mailbox_spins, &p->ctl->spins, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                             s));
-    SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
-    p->mailbox_pending = true;
-    p->last_grid = grid;
-    p->last_launches = 1;
-    p->last_lag = pp.lag;
-    p->last_nslot = pp.nslot;
-    return SRK_OK;
+// Element type of the plan's image buffers.
+template <int OP>
+srk_status launch_conv_dt(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s) {
+  switch (p->dtype) {
+    case SRK_F32: return launch_conv<OP, float>(p, a, g, conjG, s);
+    case SRK_F16: return launch_conv<OP, __half>(p, a, g, conjG, s);
+    case SRK_BF16: return launch_conv<OP, __nv_bfloat16>(p, a, g, conjG, s);
   }
-  SRK_TRY(set_smem(k_p1<M, OP, T>, sm1));
-  SRK_TRY(set_smem(k_p2<M, OP>, sm2));
-  SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
-  const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
-  int launches = 0;
-  for (int w0 = 0; w0 < nwt; w0 += chunk) {
-    const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
-    k_p1<M, OP, T><<<dim3(M / kWarps, c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
-    k_p2<M, OP><<<dim3(M / kWarps, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
-    k_p3<M, OP, T><<<dim3((g.S + kWarps - 1) / kWarps, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
-    launches += 3;
-  }
-  p->last_launches = launches;
-  return cuda_status(cudaGetLastError(), "conv launch");
-}
-
-template <int OP, typename T>
-srk_status launch_conv(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s) {
-  const int nwt = OpTraits<OP>::PAIRS ? (g.U + 1) / 2 : g.U;
-  if (nwt <= 0) return SRK_OK;
-  switch (p->M) {
-    case 128: return launch_conv_m<128, OP, T>(p, a, g, nwt, conjG, s);
-    case 256: return launch_conv_m<256, OP, T>(p, a, g, nwt, conjG, s);
-    case 512: return launch_conv_m<512, OP, T>(p, a, g, nwt, conjG, s);
-    default: return fail(SRK_ERR_UNSUPPORTED, "tile size %d not built", p->M);
-  }
+  return fail(SRK_ERR_UNSUPPORTED, "dtype %d", (int)p->dtype);
 }
 
 srk_status ensure_wbuf(srk_plan_s* p, size_t bytes, cudaStream_t s) {
@@ -221,14 +97,26 @@ srk_status ensure_wbuf(srk_plan_s* p, size_t bytes, cudaStream_t s) {
   return SRK_OK;
 }
 
-srk_status adj_wrt_f(srk_plan_s* p, const float* wx, const float* wy, const float* v, const float* ux,
-                     const float* uy, int B, float* out, cudaStream_t s) {
+template <typename T>
+void adj_wrt_f_t(srk_plan_s* p, const float* wx, const float* wy, const void* v, const void* ux, const void* uy, int B,
+                 void* out, cudaStream_t s) {
   const dim3 blk(32, 8);
   const dim3 grd((p->N + 31) / 32, (p->N + 7) / 8, B);
   if (ux)
-    k_adj_wrt_f<float, true><<<grd, blk, 0, s>>>(nullptr, nullptr, v, ux, uy, p->N, p->W, p->e, B, out);
+    k_adj_wrt_f<T, true><<<grd, blk, 0, s>>>(nullptr, nullptr, static_cast<const T*>(v), static_cast<const T*>(ux),
+                                             static_cast<const T*>(uy), p->N, p->W, p->e, B, static_cast<T*>(out));
   else
-    k_adj_wrt_f<float, false><<<grd, blk, 0, s>>>(wx, wy, nullptr, nullptr, nullptr, p->N, p->W, p->e, B, out);
+    k_adj_wrt_f<T, false><<<grd, blk, 0, s>>>(wx, wy, nullptr, nullptr, nullptr, p->N, p->W, p->e, B,
+                                              static_cast<T*>(out));
+}
+
+srk_status adj_wrt_f(srk_plan_s* p, const float* wx, const float* wy, const void* v, const void* ux,
+                     const void* uy, int B, void* out, cudaStream_t s) {
+  switch (p->dtype) {
+    case SRK_F32: adj_wrt_f_t<float>(p, wx, wy, v, ux, uy, B, out, s); break;
+    case SRK_F16: adj_wrt_f_t<__half>(p, wx, wy, v, ux, uy, B, out, s); break;
+    case SRK_BF16: adj_wrt_f_t<__nv_bfloat16>(p, wx, wy, v, ux, uy, B, out, s); break;
+  }
   return cuda_status(cudaGetLastError(), "adj_wrt_f launch");
 }
 
@@ -354,11 +242,66 @@ srk_status enter(srk_plan_s* p) {
 }
 
 // dL/dg through the adjoint engine: h = v*df (+ dv*f' for the tangent-adjoint)
-srk_status run_adj_g(srk_plan_s* p, const float* v, const float* dv, const float* f, const float* df, int B,
-                     bool conj, float* out, cudaStream_t s) {
+srk_status run_adj_g(srk_plan_s* p, const void* v, const void* dv, const void* f, const void* df, int B,
+                     bool conj, void* out, cudaStream_t s) {
   OpArgs a = base_args(p);
   a.v = v; a.dv = dv; a.I = f; a.dI = df; a.out0 = out;
-  return launch_conv<OP_ADJ, float>(p, a, adj_geom(p, B), conj, s);
+  return launch_conv_dt<OP_ADJ>(p, a, adj_geom(p, B), conj, s);
+}
+
+// ---- autotuner ------------------------------------------------------------------
+// Times every (tile size, schedule) candidate of the forward operator on
+// synthetic device data and remembers the fastest per device and
+// configuration in a small text cache (one "key value" line per entry).
+__global__ void k_fill_pattern(float* __restrict__ x, size_t n, unsigned seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned h = (unsigned)i * 2654435761u ^ seed;
+    h ^= h >> 15; h *= 2246822519u; h ^= h >> 13;
+    x[i] = (float)(h & 0xffffff) * (1.0f / 16777216.0f);
+  }
+}
+
+std::string tune_cache_path() {
+  const char* env = getenv("SRK_TUNE_CACHE");
+  if (env && *env) return env;
+  const char* home = getenv("HOME");
+  return std::string(home ? home : "/tmp") + "/.cache/srk_b200_tune.txt";
+}
+
+std::string tune_key(int N, int W, int e, int B, srk_dtype dt) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, dev);
+  std::string name(prop.name);
+  for (auto& c : name) if (c == ' ') c = '_';
+  int bb = 1;
+  while (bb < B) bb <<= 1;  // batch bucket
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s:N%d:W%d:e%d:B%d:t%d", name.c_str(), N, W, e, bb, (int)dt);
+  return buf;
+}
+
+bool tune_lookup(const std::string& key, int* M, int* sched) {
+  FILE* f = fopen(tune_cache_path().c_str(), "r");
+  if (!f) return false;
+  char k[256];
+  int m = 0, sc = 0;
+  bool found = false;
+  while (fscanf(f, "%255s %d %d", k, &m, &sc) == 3)
+    if (key == k) { *M = m; *sched = sc; found = true; }
+  fclose(f);
+  return found;
+}
+
+void tune_store(const std::string& key, int M, int sched) {
+  const std::string path = tune_cache_path();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) mkdir(path.substr(0, slash).c_str(), 0755);  // best effort
+  FILE* f = fopen(path.c_str(), "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d\n", key.c_str(), M, sched);
+  fclose(f);
 }
 
 }  // namespace
@@ -394,9 +337,14 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   if (spectra_M < 2 || (spectra_M & 1)) return fail(SRK_ERR_INVALID_ARG, "spectra_M=%d must be even", spectra_M);
   if (spectra_M < 2 * erosion + 1)
     return fail(SRK_ERR_INVALID_ARG, "spectra_M=%d smaller than the kernel support 2*erosion+1", spectra_M);
-  if (dtype != SRK_F32) return fail(SRK_ERR_UNSUPPORTED, "dtype %d: only SRK_F32 plans in this build", (int)dtype);
+  if (dtype != SRK_F32 && dtype != SRK_F16 && dtype != SRK_BF16) return fail(SRK_ERR_INVALID_ARG, "bad dtype %d", (int)dtype);
   if (!(dx > 0.f) || !std::isfinite(dx)) return fail(SRK_ERR_INVALID_ARG, "dx=%g must be positive", dx);
   int M = tile_M;
+  int sched = SRK_SCHEDULE_THREE_PASS;
+  if (M == SRK_TILE_AUTOTUNE) {
+    const srk_status st = srk_autotune(N, W, erosion, dx, B_max, dtype, &M, &sched);
+    if (st != SRK_OK) return st;
+  }
   if (M == 0) M = choose_tile(N, W, erosion);
   if (M == 0)
     return fail(SRK_ERR_UNSUPPORTED, "erosion=%d too large for the 512 tile (needs stride >= 16)", erosion);
@@ -407,6 +355,7 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   cudaGetDevice(&p->device);
   p->N = N; p->W = W; p->e = erosion; p->dx = dx; p->B_max = B_max; p->spectra_M = spectra_M; p->dtype = dtype;
   p->M = M; p->S = M - 2 * erosion;
+  p->schedule = sched;
   p->T = (W + p->S - 1) / p->S;
   p->Ta = (N + p->S - 1) / p->S;
   const size_t nwt_max = std::max<size_t>({(size_t)(B_max * (size_t)p->T * p->T + 1) / 2,
@@ -573,8 +522,12 @@ srk_status srk_precompute_kernel_freq(const float* K, int KW, int M, void* freq,
   return SRK_OK;
 }
 
-srk_status srk_training_forward(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
-                                int erosion, float dx, int B, srk_stream_t s, float* R, srk_plan p) {
+// ---- typed operator bodies (element type = plan dtype) --------------------------
+}  // extern "C"
+namespace {
+
+srk_status op_training_forward(const void* E, const void* I, const void* gx, const void* gy, int N, int W,
+                               int erosion, float dx, int B, srk_stream_t s, void* R, srk_plan p) {
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(E);
@@ -586,17 +539,11 @@ srk_status srk_training_forward(const float* E, const float* I, const void* gx, 
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R;
-  return launch_conv<OP_FWD, float>(p, a, fwd_geom(p, B), false, s);
+  return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, B), false, s);
 }
 
-srk_status srk_training_forward_sync(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
-                                     int erosion, float dx, int B, srk_stream_t s, float* R, srk_plan p) {
-  SRK_TRY(srk_training_forward(E, I, gx, gy, N, W, erosion, dx, B, s, R, p));
-  return srk_plan_sync(p, s);
-}
-
-srk_status srk_forward_oas(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
-                           int erosion, float dx, srk_stream_t s, float* R, srk_plan p, float* ux, float* uy) {
+srk_status op_forward_oas(const void* E, const void* I, const void* gx, const void* gy, int N, int W, int erosion,
+                          float dx, srk_stream_t s, void* R, srk_plan p, void* ux, void* uy) {
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(E);
   SRK_NONNULL(I);
@@ -605,12 +552,11 @@ srk_status srk_forward_oas(const float* E, const float* I, const void* gx, const
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R; a.out_ux = ux; a.out_uy = uy;
-  return launch_conv<OP_FWD, float>(p, a, fwd_geom(p, 1), false, s);
+  return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, 1), false, s);
 }
 
-srk_status srk_adjoint(const float* v, const float* ux, const float* uy, const float* I, const void* gx,
-                       const void* gy, int N, int W, int erosion, float dx, srk_stream_t s, float* dLdI, float* dLdE,
-                       srk_plan p) {
+srk_status op_adjoint(const void* v, const void* ux, const void* uy, const void* I, const void* gx, const void* gy,
+                      int N, int W, int erosion, float dx, srk_stream_t s, void* dLdI, void* dLdE, srk_plan p) {
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(v);
   SRK_NONNULL(ux);
@@ -624,8 +570,8 @@ srk_status srk_adjoint(const float* v, const float* ux, const float* uy, const f
   return run_adj_g(p, v, nullptr, I, nullptr, 1, p->conv == SRK_ADJ_TRUE, dLdE, s);
 }
 
-srk_status srk_tangent(const float* f, const float* g, const float* df, const float* dg, const void* gx,
-                       const void* gy, int N, int W, int erosion, float dx, srk_stream_t s, float* dh, srk_plan p) {
+srk_status op_tangent(const void* f, const void* g, const void* df, const void* dg, const void* gx, const void* gy,
+                      int N, int W, int erosion, float dx, srk_stream_t s, void* dh, srk_plan p) {
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);
@@ -636,12 +582,12 @@ srk_status srk_tangent(const float* f, const float* g, const float* df, const fl
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
-  return launch_conv<OP_JVP, float>(p, a, fwd_geom(p, 1), false, s);
+  return launch_conv_dt<OP_JVP>(p, a, fwd_geom(p, 1), false, s);
 }
 
-srk_status srk_tangent_adjoint(const float* f, const float* g, const float* df, const float* dg, const float* lam,
-                               const float* dlam, const void* gx, const void* gy, int N, int W, int erosion, float dx,
-                               srk_stream_t s, float* dLam_f, float* dLam_g, srk_plan p) {
+srk_status op_tangent_adjoint(const void* f, const void* g, const void* df, const void* dg, const void* lam,
+                              const void* dlam, const void* gx, const void* gy, int N, int W, int erosion, float dx,
+                              srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);
@@ -657,12 +603,12 @@ srk_status srk_tangent_adjoint(const float* f, const float* g, const float* df, 
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.v = lam; a.dv = dlam; a.out0 = p->wbuf; a.out1 = p->wbuf + ww;
-  SRK_TRY((launch_conv<OP_TANADJ_F, float>(p, a, fwd_geom(p, 1), false, s)));
+  SRK_TRY(launch_conv_dt<OP_TANADJ_F>(p, a, fwd_geom(p, 1), false, s));
   SRK_TRY(adj_wrt_f(p, p->wbuf, p->wbuf + ww, nullptr, nullptr, nullptr, 1, dLam_f, s));
   return run_adj_g(p, lam, dlam, f, df, 1, p->conv == SRK_ADJ_TRUE, dLam_g, s);
 }
 
-srk_status srk_forward(const float* f, const float* g, int B, srk_stream_t s, float* h, srk_plan p) {
+srk_status op_forward(const void* f, const void* g, int B, srk_stream_t s, void* h, srk_plan p) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(f);
@@ -672,11 +618,11 @@ srk_status srk_forward(const float* f, const float* g, int B, srk_stream_t s, fl
   SRK_TRY(enter(p));
   OpArgs a = base_args(p);
   a.E = g; a.I = f; a.out0 = h;
-  return launch_conv<OP_FWD, float>(p, a, fwd_geom(p, B), false, s);
+  return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, B), false, s);
 }
 
-srk_status srk_vjp(const float* v, const float* f, const float* g, int B, srk_stream_t s, float* dLdf, float* dLdg,
-                   srk_plan p) {
+srk_status op_vjp(const void* v, const void* f, const void* g, int B, srk_stream_t s, void* dLdf, void* dLdg,
+                  srk_plan p) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(v);
@@ -690,14 +636,14 @@ srk_status srk_vjp(const float* v, const float* f, const float* g, int B, srk_st
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
   OpArgs a = base_args(p);
   a.E = g; a.v = v; a.out0 = p->wbuf; a.out1 = p->wbuf + ww;
-  SRK_TRY((launch_conv<OP_VJP_F, float>(p, a, fwd_geom(p, B), false, s)));
-  // k_adj_wrt_f expects per-image wx, wy planes: [B][W][W] each
+  SRK_TRY(launch_conv_dt<OP_VJP_F>(p, a, fwd_geom(p, B), false, s));
+  // per-image wx, wy planes: [B][W][W] each
   SRK_TRY(adj_wrt_f(p, p->wbuf, p->wbuf + ww, nullptr, nullptr, nullptr, B, dLdf, s));
   return run_adj_g(p, v, nullptr, f, nullptr, B, true, dLdg, s);
 }
 
-srk_status srk_jvp(const float* f, const float* g, const float* df, const float* dg, int B, srk_stream_t s,
-                   float* dh, srk_plan p) {
+srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, int B, srk_stream_t s, void* dh,
+                  srk_plan p) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(f);
@@ -709,7 +655,173 @@ srk_status srk_jvp(const float* f, const float* g, const float* df, const float*
   SRK_TRY(enter(p));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
-  return launch_conv<OP_JVP, float>(p, a, fwd_geom(p, B), false, s);
+  return launch_conv_dt<OP_JVP>(p, a, fwd_geom(p, B), false, s);
+}
+
+// The float* entry points are the reference drop-ins: fp32 plans only.
+srk_status need_f32(srk_plan p) {
+  if (p && p->dtype != SRK_F32)
+    return fail(SRK_ERR_INVALID_ARG, "this entry point takes float buffers; the plan stores dtype %d (use the _t form)",
+                (int)p->dtype);
+  return SRK_OK;
+}
+
+}  // namespace
+extern "C" {
+
+srk_status srk_training_forward(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
+                                int erosion, float dx, int B, srk_stream_t s, float* R, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_training_forward(E, I, gx, gy, N, W, erosion, dx, B, s, R, p);
+}
+
+srk_status srk_training_forward_sync(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
+                                     int erosion, float dx, int B, srk_stream_t s, float* R, srk_plan p) {
+  SRK_TRY(srk_training_forward(E, I, gx, gy, N, W, erosion, dx, B, s, R, p));
+  return srk_plan_sync(p, s);
+}
+
+srk_status srk_forward_oas(const float* E, const float* I, const void* gx, const void* gy, int N, int W,
+                           int erosion, float dx, srk_stream_t s, float* R, srk_plan p, float* ux, float* uy) {
+  SRK_TRY(need_f32(p));
+  return op_forward_oas(E, I, gx, gy, N, W, erosion, dx, s, R, p, ux, uy);
+}
+
+srk_status srk_adjoint(const float* v, const float* ux, const float* uy, const float* I, const void* gx,
+                       const void* gy, int N, int W, int erosion, float dx, srk_stream_t s, float* dLdI, float* dLdE,
+                       srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_adjoint(v, ux, uy, I, gx, gy, N, W, erosion, dx, s, dLdI, dLdE, p);
+}
+
+srk_status srk_tangent(const float* f, const float* g, const float* df, const float* dg, const void* gx,
+                       const void* gy, int N, int W, int erosion, float dx, srk_stream_t s, float* dh, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent(f, g, df, dg, gx, gy, N, W, erosion, dx, s, dh, p);
+}
+
+srk_status srk_tangent_adjoint(const float* f, const float* g, const float* df, const float* dg, const float* lam,
+                               const float* dlam, const void* gx, const void* gy, int N, int W, int erosion, float dx,
+                               srk_stream_t s, float* dLam_f, float* dLam_g, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent_adjoint(f, g, df, dg, lam, dlam, gx, gy, N, W, erosion, dx, s, dLam_f, dLam_g, p);
+}
+
+srk_status srk_forward(const float* f, const float* g, int B, srk_stream_t s, float* h, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_forward(f, g, B, s, h, p);
+}
+
+srk_status srk_vjp(const float* v, const float* f, const float* g, int B, srk_stream_t s, float* dLdf, float* dLdg,
+                   srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_vjp(v, f, g, B, s, dLdf, dLdg, p);
+}
+
+srk_status srk_jvp(const float* f, const float* g, const float* df, const float* dg, int B, srk_stream_t s,
+                   float* dh, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_jvp(f, g, df, dg, B, s, dh, p);
+}
+
+// ---- storage-typed forms: element type of every image buffer = plan dtype ------
+srk_status srk_training_forward_t(const void* E, const void* I, const void* gx, const void* gy, int N, int W,
+                                  int erosion, float dx, int B, srk_stream_t s, void* R, srk_plan p) {
+  return op_training_forward(E, I, gx, gy, N, W, erosion, dx, B, s, R, p);
+}
+srk_status srk_forward_oas_t(const void* E, const void* I, const void* gx, const void* gy, int N, int W, int erosion,
+                             float dx, srk_stream_t s, void* R, srk_plan p, void* ux, void* uy) {
+  return op_forward_oas(E, I, gx, gy, N, W, erosion, dx, s, R, p, ux, uy);
+}
+srk_status srk_adjoint_t(const void* v, const void* ux, const void* uy, const void* I, const void* gx, const void* gy,
+                         int N, int W, int erosion, float dx, srk_stream_t s, void* dLdI, void* dLdE, srk_plan p) {
+  return op_adjoint(v, ux, uy, I, gx, gy, N, W, erosion, dx, s, dLdI, dLdE, p);
+}
+srk_status srk_tangent_t(const void* f, const void* g, const void* df, const void* dg, const void* gx, const void* gy,
+                         int N, int W, int erosion, float dx, srk_stream_t s, void* dh, srk_plan p) {
+  return op_tangent(f, g, df, dg, gx, gy, N, W, erosion, dx, s, dh, p);
+}
+srk_status srk_tangent_adjoint_t(const void* f, const void* g, const void* df, const void* dg, const void* lam,
+                                 const void* dlam, const void* gx, const void* gy, int N, int W, int erosion,
+                                 float dx, srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
+  return op_tangent_adjoint(f, g, df, dg, lam, dlam, gx, gy, N, W, erosion, dx, s, dLam_f, dLam_g, p);
+}
+srk_status srk_forward_t(const void* f, const void* g, int B, srk_stream_t s, void* h, srk_plan p) {
+  return op_forward(f, g, B, s, h, p);
+}
+srk_status srk_vjp_t(const void* v, const void* f, const void* g, int B, srk_stream_t s, void* dLdf, void* dLdg,
+                     srk_plan p) {
+  return op_vjp(v, f, g, B, s, dLdf, dLdg, p);
+}
+srk_status srk_jvp_t(const void* f, const void* g, const void* df, const void* dg, int B, srk_stream_t s, void* dh,
+                     srk_plan p) {
+  return op_jvp(f, g, df, dg, B, s, dh, p);
+}
+
+srk_status srk_autotune(int N, int W, int erosion, float dx, int B, srk_dtype dtype, int* tile_M, int* schedule) {
+  if (!tile_M || !schedule) return fail(SRK_ERR_INVALID_ARG, "NULL output pointer");
+  if (N < 3 || erosion < 0 || W != N - 2 * erosion || W < 1 || B < 1)
+    return fail(SRK_ERR_INVALID_ARG, "bad sizes for autotune (N=%d W=%d erosion=%d B=%d)", N, W, erosion, B);
+  const std::string key = tune_key(N, W, erosion, B, dtype);
+  if (tune_lookup(key, tile_M, schedule)) return SRK_OK;
+  // synthetic workload: a smooth Green's tensor and uniform images
+  const int KW = 2 * erosion + 1;
+  const int Bt = B < 512 ? B : 512;
+  const size_t esz = dtype == SRK_F32 ? 4 : 2;
+  cudaStream_t s = nullptr;
+  SRK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  float *Kx = nullptr, *Ky = nullptr;
+  void *E = nullptr, *R = nullptr;
+  srk_status st = SRK_OK;
+  float best = 0.f;
+  int bestM = 0, bestS = SRK_SCHEDULE_THREE_PASS;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto done = [&](srk_status r) {
+    if (Kx) cudaFree(Kx);
+    if (Ky) cudaFree(Ky);
+    if (E) cudaFree(E);
+    if (R) cudaFree(R);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    return r;
+  };
+  if (cudaMalloc(&Kx, sizeof(float) * KW * KW) != cudaSuccess || cudaMalloc(&Ky, sizeof(float) * KW * KW) != cudaSuccess ||
+      cudaMalloc(&E, esz * (size_t)Bt * N * N) != cudaSuccess || cudaMalloc(&R, esz * (size_t)Bt * W * W) != cudaSuccess)
+    return done(fail(SRK_ERR_ALLOC, "autotune buffers"));
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  if ((st = srk_green_tensor(Kx, Ky, KW, 1.0 / (erosion / 3.0 + 1.0), (double)erosion + 0.5, 1.0, s)) != SRK_OK)
+    return done(st);
+  // any bit pattern is a valid half input too; the values only need to be finite
+  k_fill_pattern<<<256, 256, 0, s>>>(static_cast<float*>(E), esz * (size_t)Bt * N * N / 4, 1234u);
+  if (dtype != SRK_F32) SRK_CUDA(cudaMemsetAsync(E, 0, esz * (size_t)Bt * N * N, s));
+  const int cand[3] = {128, 256, 512};
+  for (int M : cand) {
+    if (M - 2 * erosion < 16) continue;
+    for (int sch = 0; sch < 2; ++sch) {
+      srk_plan p = nullptr;
+      if (srk_plan_create(&p, N, W, erosion, dx, Bt, N + (N & 1), dtype, M, 0) != SRK_OK) continue;
+      p->schedule = sch;
+      p->persist_prefetch = 0;
+      if ((st = srk_plan_set_kernel(p, Kx, Ky, KW, s)) != SRK_OK) { srk_plan_destroy(p); return done(st); }
+      for (int it = 0; it < 2; ++it) op_forward(E, E, Bt, s, R, p);
+      cudaEventRecord(e0, s);
+      for (int it = 0; it < 3; ++it) op_forward(E, E, Bt, s, R, p);
+      cudaEventRecord(e1, s);
+      st = srk_plan_sync(p, s);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      srk_plan_destroy(p);
+      if (st != SRK_OK) return done(st);
+      if (bestM == 0 || ms < best) { best = ms; bestM = M; bestS = sch; }
+    }
+  }
+  if (bestM == 0) return done(fail(SRK_ERR_UNSUPPORTED, "no tile size fits erosion=%d", erosion));
+  *tile_M = bestM;
+  *schedule = bestS;
+  tune_store(key, bestM, bestS);
+  return done(SRK_OK);
 }
 
 }  // extern "C"

@@ -58,8 +58,8 @@ def test_plan_create_rejects_unbuilt_tile_and_dtype():
         srk.SrkPlan(256, 226, 15, 1.0, 1, 256, tile_M=1024)
     assert ei.value.status == srk.SRK_ERR_INVALID_ARG
     with pytest.raises(srk.SrkError) as ei:
-        srk.SrkPlan(256, 226, 15, 1.0, 1, 256, dtype=srk.SRK_F16)
-    assert ei.value.status == srk.SRK_ERR_UNSUPPORTED
+        srk.SrkPlan(256, 226, 15, 1.0, 1, 256, dtype=7)
+    assert ei.value.status == srk.SRK_ERR_INVALID_ARG
     with pytest.raises(srk.SrkError) as ei:  # erosion too large for any tile
         srk.SrkPlan(2048, 2048 - 2 * 300, 300, 1.0, 1, 2048)
     assert ei.value.status == srk.SRK_ERR_UNSUPPORTED

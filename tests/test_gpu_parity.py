@@ -270,3 +270,80 @@ def test_bounded_wait_gives_up_and_context_survives(torch_cuda):
     srk.srkTrainingForward(E, E, GX, GY, 128, 98, 15, 1.0, 2, None, R, plan)
     plan.sync()
     assert rel_max_err(host(R)[0], O.forward(host(E)[0], host(E)[0], Kx, Ky, 15, 1.0)) < 1e-3
+
+
+@pytest.mark.parametrize("dtype", ["f16", "bf16"])
+@pytest.mark.parametrize("N,KW,B", [(256, 31, 3), (512, 121, 2)])
+def test_half_storage_training_forward(torch_cuda, dtype, N, KW, B):
+    """FP16/BF16 storage, FP32 arithmetic: within rel 1e-2 / abs 1e-3 of the
+    FP64 oracle on the same (rounded) inputs."""
+    torch = torch_cuda
+    tdt = torch.float16 if dtype == "f16" else torch.bfloat16
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    Kx, Ky = kernel(KW, "baseline", 4.0)
+    GX, GY = spectra(Kx, Ky, N, torch)
+    E = dev(np.stack(fields(N, B, 70 + N)), torch).to(tdt)
+    plan = srk.SrkPlan(N, W, e, 4.0, B, dtype=srk.SRK_F16 if dtype == "f16" else srk.SRK_BF16)
+    R = torch.zeros((B, W, W), device="cuda", dtype=tdt)
+    srk.srkTrainingForward(E, E, GX, GY, N, W, e, 4.0, B, None, R, plan)
+    plan.sync()
+    Eh = E.float().cpu().numpy().astype(np.float64)
+    Rh = R.float().cpu().numpy().astype(np.float64)
+    for b in range(B):
+        ref = O.forward(Eh[b], Eh[b], Kx, Ky, e, 4.0)
+        assert rel_max_err(Rh[b], ref) < 1e-2
+        assert pixel_violations(Rh[b], ref, tol_abs=1e-3, tol_rel=1e-2) == 0
+
+
+@pytest.mark.parametrize("dtype", ["f16", "bf16"])
+def test_half_storage_derivatives(torch_cuda, dtype):
+    torch = torch_cuda
+    tdt = torch.float16 if dtype == "f16" else torch.bfloat16
+    N, KW = 300, 31
+    e = 15
+    W = N - 2 * e
+    Kx, Ky = kernel(KW)
+    GX, GY = spectra(Kx, Ky, 1024, torch)
+    f, g = fields(N, 2, 801)
+    rng = np.random.default_rng(5)
+    df, dg = [(1e-2 * rng.standard_normal((N, N))).astype(np.float32) for _ in range(2)]
+    lam, dlam = [rng.standard_normal((W, W)).astype(np.float32) for _ in range(2)]
+    hp = lambda a: dev(a, torch).to(tdt)
+    back = lambda t: t.float().cpu().numpy().astype(np.float64)
+    F, G, DF, DG, LAM, DLAM = [hp(a) for a in (f, g, df, dg, lam, dlam)]
+    fh, gh, dfh, dgh, lamh, dlamh = [back(t) for t in (F, G, DF, DG, LAM, DLAM)]
+    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=1024, tile_M=128,
+                       dtype=srk.SRK_F16 if dtype == "f16" else srk.SRK_BF16)
+    dh = torch.zeros((W, W), device="cuda", dtype=tdt)
+    srk.shrinkageTangentOaS(F, G, DF, DG, GX, GY, N, W, e, 1.0, None, dh, plan)
+    dlf = torch.zeros((N, N), device="cuda", dtype=tdt)
+    dlg = torch.zeros((N, N), device="cuda", dtype=tdt)
+    srk.shrinkageTangentAdjointOaS(F, G, DF, DG, LAM, DLAM, GX, GY, N, W, e, 1.0, None, dlf, dlg, plan)
+    plan.sync()
+    assert rel_max_err(back(dh), O.tangent(fh, gh, dfh, dgh, Kx, Ky, e, 1.0)) < 1e-2
+    of, og = O.tangent_adjoint(fh, gh, dfh, dgh, lamh, dlamh, Kx, Ky, e, 1.0, "reference")
+    assert rel_max_err(back(dlf), of) < 1e-2
+    assert rel_max_err(back(dlg), og) < 1e-2
+
+
+def test_autotuned_plan_is_correct_and_cached(torch_cuda, tmp_path, monkeypatch):
+    torch = torch_cuda
+    monkeypatch.setenv("SRK_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    N, KW, B = 256, 31, 4
+    e = 15
+    W = N - 2 * e
+    M, sch = srk.autotune(N, W, e, 1.0, B)
+    assert M in (128, 256, 512) and sch in (0, 1)
+    lines = (tmp_path / "tune.txt").read_text().split("\n")
+    assert any(l.endswith(" %d %d" % (M, sch)) for l in lines)
+    assert srk.autotune(N, W, e, 1.0, B) == (M, sch)  # from the cache
+    plan = srk.SrkPlan(N, W, e, 1.0, B, tile_M=srk.SRK_TILE_AUTOTUNE)
+    assert plan.info()["tile_M"] == M and plan.info()["schedule"] == sch
+    Kx, Ky = kernel(KW)
+    GX, GY = spectra(Kx, Ky, N, torch)
+    E = dev(np.stack(fields(N, B, 3)), torch)
+    R = torch.zeros((B, W, W), device="cuda")
+    srk.srkTrainingForward(E, E, GX, GY, N, W, e, 1.0, B, None, R, plan)
+    plan.sync()
+    assert rel_max_err(host(R)[1], O.forward(host(E)[1], host(E)[1], Kx, Ky, e, 1.0)) < 1e-3
