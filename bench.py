@@ -36,8 +36,8 @@ sys.path.insert(0, ROOT)
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--steps", type=int, default=60)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--B", type=int, default=5000)
     p.add_argument("--N", type=int, default=512)
@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ops", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the fp16 and published-config lines")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     return p.parse_args()
 
@@ -263,11 +264,11 @@ def run_ours(a):
     _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
     E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17)
     R = torch.empty((B, W, W), device="cuda")
-    plan = srk.SrkPlan(N, W, e, dx, B)
-    info = plan.info()
+    plan = srk.SrkPlan(N, W, e, dx, B, tile_M=srk.SRK_TILE_AUTOTUNE)
     step = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
     step()
-    torch.cuda.synchronize()
+    plan.sync()
+    info = plan.info()
 
     clk = ClockSampler(local)
     clk.start()
@@ -277,8 +278,7 @@ def run_ours(a):
     imgs_per_s = world * B / (ms * 1e-3)
     mpix = world * B * W * W / (ms * 1e-3) / 1e6
 
-    nwt = (B * info["tiles"] ** 2 + 1) // 2
-    launches_per_step = 3 * ((nwt + info["chunk_wt"] - 1) // info["chunk_wt"])
+    launches_per_step = info["last_launches"]
     peak, peak_kind = measured_peaks()
     alg_bytes = B * (N * N + W * W) * 4
     achieved = alg_bytes / (ms * 1e-3) / 1e9
@@ -295,6 +295,11 @@ def run_ours(a):
     ops = None
     if not a.no_ops and world == 1:
         ops = ops_throughput(torch, srk)
+
+    extra = {}
+    if not a.no_extra and world == 1:
+        extra["fp16_storage"] = half_storage_rate(torch, srk, E, GX, GY, N, W, e, dx, B)
+        extra["published_config"] = published_config_rate(torch, srk)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -323,10 +328,49 @@ def run_ours(a):
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
+            "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass"][info["schedule"]],
+                         "autotuned": True},
         }
+        line.update(extra)
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def half_storage_rate(torch, srk, E32, GX, GY, N, W, e, dx, B, steps=20):
+    """Same workload with FP16 image storage (FP32 arithmetic)."""
+    E = E32.half()
+    R = torch.empty((B, W, W), device="cuda", dtype=torch.float16)
+    plan = srk.SrkPlan(N, W, e, dx, B, dtype=srk.SRK_F16, tile_M=srk.SRK_TILE_AUTOTUNE)
+    fn = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
+    ms = time_steps(torch, fn, steps, 3, None)
+    peak, _ = measured_peaks()
+    alg = B * (N * N + W * W) * 2
+    out = {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "dtype": "f16 storage, f32 arithmetic",
+           "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "tile_M": plan.info()["tile_M"]}
+    del E, R, plan
+    torch.cuda.empty_cache()
+    return out
+
+
+def published_config_rate(torch, srk, steps=20):
+    """The only published number of the reference: srkTrainingForward at
+    B=3000, N=256, KW=121 took 55.39 ms on an sm_86-class GPU
+    (notebooks/plot_compare_demo.ipynb cell 0)."""
+    B, N, KW = 3000, 256, 121
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    _, _, GX, GY = make_spectra(torch, srk, KW, N, 1.0)
+    E = grf_batch(torch, B, N, 99)
+    R = torch.empty((B, W, W), device="cuda")
+    plan = srk.SrkPlan(N, W, e, 1.0, B, tile_M=srk.SRK_TILE_AUTOTUNE)
+    fn = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, 1.0, B, None, R, plan)
+    ms = time_steps(torch, fn, steps, 3, None)
+    out = {"config": "B=3000 N=256 KW=121", "ms_per_step": ms, "value": B / (ms * 1e-3), "unit": "img/s",
+           "published_ms": 55.39, "speedup_vs_published": 55.39 / ms, "tile_M": plan.info()["tile_M"]}
+    del E, R, plan
+    torch.cuda.empty_cache()
+    return out
 
 
 def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
@@ -338,7 +382,7 @@ def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
     f, g = grf_batch(torch, 2, N, 77)
     df, dg = (1e-2 * torch.randn((2, N, N), device="cuda")).unbind(0)
     lam, dlam = torch.randn((2, W, W), device="cuda").unbind(0)
-    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=1024)
+    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=1024, tile_M=srk.SRK_TILE_AUTOTUNE)
     R = torch.empty((W, W), device="cuda")
     ux, uy = torch.empty_like(R), torch.empty_like(R)
     o1, o2 = torch.empty((N, N), device="cuda"), torch.empty((N, N), device="cuda")
@@ -354,7 +398,7 @@ def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
            "tangent": 4 * N * N + W * W, "tangent_adjoint": 6 * N * N + 2 * W * W}
     peak, _ = measured_peaks()
     for k, fn in runs.items():
-        ms = time_steps(torch, fn, reps, 2, None)
+        ms = time_steps(torch, fn, reps * 4, 2, None)
         px = W * W if k in ("forward", "tangent") else N * N
         out[k] = {"ms": ms, "out_mpix_per_s": px / (ms * 1e-3) / 1e6,
                   "hbm_frac": alg[k] * 4 / (ms * 1e-3) / 1e9 / peak}

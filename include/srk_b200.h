@@ -188,6 +188,22 @@ srk_status srk_vjp(const float* d_v, const float* d_f, const float* d_g, int B, 
 srk_status srk_jvp(const float* d_f, const float* d_g, const float* d_df, const float* d_dg, int B,
                    srk_stream_t stream, float* d_dh, srk_plan plan);
 
+/* ---- critical dimension (CD) of line/space signals ------------------------
+ * MeasureCD_Batched (third_party/src/metricUtil/cd_measure_util.cu:310-437)
+ * in one kernel per signal: L-fold windowed-sinc upsampling (half width A),
+ * sub-sample zero crossings, nearest crossing left of the centre and at or
+ * right of it; d_left, d_right, d_cd [B] in input pixels, written on the
+ * device (no host synchronisation).  Signals are d_sig [B][n], n <= 8192. */
+srk_status srk_measure_cd(const float* d_sig, int B, int n, int L, int A, srk_stream_t stream, float* d_left,
+                          float* d_right, float* d_cd);
+/* CD of the centre line of E_crop + coeff*R (axis 0: centre row, axis 1:
+ * centre column), E [B][N][N], R [B][W][W] from srk_training_forward: the
+ * crop / apply_shrinkage / extract / measure sequence of
+ * training/main_cd_training.cu:193-261 fused into the same kernel. */
+srk_status srk_cd_after_shrinkage(const float* d_E, const float* d_R, int B, int N, int W, int erosion, float coeff,
+                                  int axis, int L, int A, srk_stream_t stream, float* d_left, float* d_right,
+                                  float* d_cd);
+
 /* ---- storage-typed forms ----------------------------------------------------
  * Same operators with every image / cotangent / output buffer in the plan's
  * storage type (SRK_F32: float, SRK_F16: IEEE half, SRK_BF16: bfloat16),

@@ -66,6 +66,8 @@ _SIGS = {
     "srk_plan_get_info": [_P, ctypes.POINTER(PlanInfo)],
     "srk_plan_set_adj_convention": [_P, _I],
     "srk_plan_set_schedule": [_P, _I],
+    "srk_measure_cd": [_P, _I, _I, _I, _I, _P, _P, _P, _P],
+    "srk_cd_after_shrinkage": [_P, _P, _I, _I, _I, _I, _F, _I, _I, _I, _P, _P, _P, _P],
     "srk_autotune": [_I, _I, _I, _F, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "srk_plan_set_persistent": [_P, _I, _I, _I],
     "srk_plan_sync": [_P, _P],
@@ -254,3 +256,23 @@ def vjp(v, f, g, B, dLdf, dLdg, ws, stream=None):
 
 def jvp(f, g, df, dg, B, dh, ws, stream=None):
     _check(_entry("srk_jvp", ws)(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), B, _stream(stream), _ptr(dh), ws.handle))
+
+
+def measure_cd(sig, L=16, A=8, stream=None):
+    """(left, right, cd) device tensors [B] for signals sig [B][n]
+    (MeasureCD_Batched semantics, pixels)."""
+    import torch
+    B, n = sig.shape
+    out = [torch.empty(B, device=sig.device, dtype=torch.float32) for _ in range(3)]
+    _check(lib().srk_measure_cd(_ptr(sig), B, n, L, A, _stream(stream), *[_ptr(t) for t in out]))
+    return tuple(out)
+
+
+def cd_after_shrinkage(E, R, N, W, erosion, coeff, axis, L=16, A=8, stream=None):
+    """CD of the centre row (axis 0) or column (axis 1) of E_crop + coeff*R."""
+    import torch
+    B = E.shape[0]
+    out = [torch.empty(B, device=E.device, dtype=torch.float32) for _ in range(3)]
+    _check(lib().srk_cd_after_shrinkage(_ptr(E), _ptr(R), B, N, W, erosion, coeff, axis, L, A, _stream(stream),
+                                        *[_ptr(t) for t in out]))
+    return tuple(out)

@@ -68,7 +68,7 @@ struct srk_plan_s {
   bool mailbox_pending = false;
   unsigned long long spin_limit = 1ull << 25;
   unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
-  int persist_lag = 0, persist_grid = 0, persist_prefetch = 1;
+  int persist_lag = 0, persist_grid = 0, persist_prefetch = 0;
   int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
 };
 
