@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--no-ops", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the fp16 and published-config lines")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass"],
+                   help="override the autotuned kernel schedule (profiling)")
     return p.parse_args()
 
 
@@ -265,6 +267,8 @@ def run_ours(a):
     E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17)
     R = torch.empty((B, W, W), device="cuda")
     plan = srk.SrkPlan(N, W, e, dx, B, tile_M=srk.SRK_TILE_AUTOTUNE)
+    if a.schedule != "auto":
+        plan.set_schedule(srk.SRK_SCHEDULE_PERSISTENT if a.schedule == "persistent" else srk.SRK_SCHEDULE_THREE_PASS)
     step = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
     step()
     plan.sync()
@@ -329,7 +333,7 @@ def run_ours(a):
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
             "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass"][info["schedule"]],
-                         "autotuned": True},
+                         "autotuned": a.schedule == "auto"},
         }
         line.update(extra)
         print(json.dumps(line))

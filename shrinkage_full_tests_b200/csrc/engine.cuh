@@ -42,6 +42,10 @@
 
 namespace srk {
 
+constexpr int kWarps = 8;
+constexpr int kThreads = 32 * kWarps;
+constexpr int kThreadsStage = kThreads;
+
 enum Op : int {
   OP_FWD = 0,       // R = ux*df/dx + uy*df/dy (pairs of tiles); optional ux/uy
   OP_VJP_F = 1,     // wx = ux*v, wy = uy*v (pairs of tiles) for dL/df
@@ -374,9 +378,87 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
   }
 }
 
+// ---- staged gradients -------------------------------------------------------------
+// The 8 output columns of a P3 unit need the image columns gx-1 .. gx+8 and
+// rows gy-1 .. gy+S.  They are staged cooperatively (coalesced, every load
+// in flight) into shared memory: window column c <-> image column
+// x0 + e - 1 + c, window row r <-> image row y0 + e - 1 + r; out-of-image
+// elements are zero (the central-difference rule).
+__host__ __device__ inline int gwin_pitch(int S) { return (S + 2 + 1) & ~1; }
+// 10 * gwin_pitch(S) floats <= 10 * (M + 3) <= 16 * (M + M/16 + 2): one
+// image's window always fits the 8 staging rows of the second field.
+
+template <typename T>
+__device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int N, int gx0, int gy0, int S,
+                                                  float* __restrict__ dst) {
+  const int HP = gwin_pitch(S);
+  const int H = S + 2;
+  for (int idx = threadIdx.x; idx < 10 * H; idx += kThreadsStage) {
+    const int c = idx / H, r = idx - (idx / H) * H;
+    const int gx = gx0 + c, gy = gy0 + r;
+    dst[c * HP + r] = (gx >= 0 && gx < N && gy >= 0 && gy < N) ? ldf(img, (long long)gx * N + gy) : 0.f;
+  }
+}
+
+// Forward / tangent epilogue, round h, with the central differences read
+// from the staged window (window column warp+1 is this warp's image column).
+// FWD: round h finishes image h of the pair.  JVP: round 0 (window = f)
+// leaves the f terms in z0[i].y, round 1 (window = df) adds the df terms.
+// z0 stays stashed in the warp's row (z0s = its padded row, element i at
+// z0s[34 i]) to keep registers for the window reads.
+template <int M, int OP, typename T>
+__device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, int w, int x, int warp, int lane,
+                                                int h, float2* __restrict__ z0s, const float2 (&z1)[M / 32],
+                                                const float* __restrict__ win, int HP) {
+  constexpr int EPT = M / 32;
+  const int W = a.W;
+  const int rb = lane - g.e + 1;  // window row of element 0: y - e + 1, y = lane
+  const float* cm = win + warp * HP + rb;  // image column gx - 1
+  const float* cc = cm + HP;               // gx
+  const float* cp = cc + HP;               // gx + 1
+  const TileRef t = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+  const int ox = t.x0 + x - g.e;
+  if (!t.live || ox >= g.Wout) return;
+  const unsigned vm = valid_rows<M>(g, t.y0, lane);
+  const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+  if constexpr (OP == OP_FWD) {
+    T* __restrict__ R = static_cast<T*>(a.out0);
+    T* __restrict__ UX = static_cast<T*>(a.out_ux);
+    T* __restrict__ UY = static_cast<T*>(a.out_uy);
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      if (!(vm >> i & 1u)) continue;
+      const float2 z0i = z0s[34 * i];
+      const float ux = h ? z0i.y : z0i.x;
+      const float uy = h ? z1[i].y : z1[i].x;
+      if (UX) stf(UX, ob + 32 * i, ux);
+      if (UY) stf(UY, ob + 32 * i, uy);
+      if (R) {
+        const float fx = (cp[32 * i] - cm[32 * i]) * 0.5f;
+        const float fy = (cc[32 * i + 1] - cc[32 * i - 1]) * 0.5f;
+        stf(R, ob + 32 * i, ux * fx + uy * fy);
+      }
+    }
+  } else {
+    // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52):
+    // dh = Im(zx) fx + Im(zy) fy + Re(zx) dfx + Re(zy) dfy
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      if (!(vm >> i & 1u)) continue;
+      const float dx_ = (cp[32 * i] - cm[32 * i]) * 0.5f;
+      const float dy_ = (cc[32 * i + 1] - cc[32 * i - 1]) * 0.5f;
+      float2 z0i = z0s[34 * i];
+      if (h == 0) {
+        z0i.y = z0i.y * dx_ + z1[i].y * dy_;
+        z0s[34 * i] = z0i;
+      } else {
+        stf(static_cast<T*>(a.out0), ob + 32 * i, z0i.y + z0i.x * dx_ + z1[i].x * dy_);
+      }
+    }
+  }
+}
+
 // ---- phases ------------------------------------------------------------------
-constexpr int kWarps = 8;
-constexpr int kThreads = 32 * kWarps;
 
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int M) {
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
@@ -516,7 +598,10 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
 }
 
 // P3: columns x' = xb*8 .. +7: stage them, inverse FFT along ky, epilogue.
-// All threads of the CTA take part.
+// All threads of the CTA take part (warps without a valid column still join
+// the barriers).  For the forward and tangent epilogues with erosion >= 1
+// the image columns the central differences need are staged in shared
+// memory after the transforms, in the rows the transforms no longer use.
 template <int M, int OP, typename T>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int warp,
@@ -524,28 +609,54 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   constexpr int EPT = M / 32;
   constexpr int L = OpTraits<OP>::L;
   constexpr int RS = row_stride<M>();
+  constexpr bool GRAD = (OP == OP_FWD || OP == OP_JVP);
   const int P = s2_pitch(g.S);
   const int x0 = xb * kWarps;
 #pragma unroll
   for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * kWarps * RS);
   __syncthreads();
   const int xv = x0 + warp;
-  if (xv >= g.S) return;
+  const bool active = xv < g.S;
   float2* row0 = rows + warp * RS;
   float2* row1 = rows + (kWarps + warp) * RS;
   float2 z0[EPT], z1[EPT];
-  row_to_regs<M>(row0, z0, lane);
-  fft<M, true>(z0, row0, tw, lane);
-  if constexpr (L == 2) {
-    __syncwarp();
-    regs_to_row<M>(row0, z0, lane);   // stash, reload after the second transform
-    row_to_regs<M>(row1, z1, lane);
-    fft<M, true>(z1, row1, tw, lane);
-    __syncwarp();
+  if (active) {
     row_to_regs<M>(row0, z0, lane);
-  } else {
+    fft<M, true>(z0, row0, tw, lane);
+    if constexpr (L == 2) {
+      __syncwarp();
+      regs_to_row<M>(row0, z0, lane);   // stash, reload after the second transform
+      row_to_regs<M>(row1, z1, lane);
+      fft<M, true>(z1, row1, tw, lane);
+    }
+  }
+  if constexpr (L == 1) {
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z1[i] = make_float2(0.f, 0.f);
+  }
+  if constexpr (GRAD) {
+    if (a.e >= 1) {
+      // two rounds, one image window each, in the row1 block
+      float* win = reinterpret_cast<float*>(rows + kWarps * RS);
+      const int HP = gwin_pitch(g.S);
+      float2* z0s = row0 + lane + (lane >> 4);
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        __syncthreads();  // row1 no longer used (round 0) / window consumed (round 1)
+        const TileRef t = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+        const T* img = static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI);
+        if (t.live)
+          stage_grad_window<T>(img + (long long)t.b * a.N * a.N, a.N, t.x0 + x0 + a.e - 1, t.y0 + a.e - 1, g.S, win);
+        __syncthreads();
+        if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, warp, lane, h, z0s, z1, win, HP);
+      }
+      return;
+    }
+  }
+  if (!active) return;
+  if constexpr (L == 2) {
+    __syncwarp();
+    row_to_regs<M>(row0, z0, lane);
   }
   epilogue_column<M, OP, T>(a, g, w, xv + g.e, lane, z0, z1);
 }
