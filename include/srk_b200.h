@@ -204,6 +204,22 @@ srk_status srk_cd_after_shrinkage(const float* d_E, const float* d_R, int B, int
                                   int axis, int L, int A, srk_stream_t stream, float* d_left, float* d_right,
                                   float* d_cd);
 
+/* ---- training forward without any device allocation ---------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (code running inside another framework's memory pool or under a fixed
+ * memory budget, plug-ins whose host owns every allocation, paths where an
+ * allocation could synchronise the device): same arguments and result as
+ * srk_training_forward, but no plan and no allocation of any kind — all
+ * scratch lives in one 32 MiB array compiled into the library (held by every
+ * GPU that loads it until the process exits).  N must be 128, 256 or 512 and
+ * the spectra are at size N.  The first call on a device resolves the
+ * array's device address; make it outside any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised. */
+srk_status srk_training_forward_noalloc(const float* d_E, const float* d_I, const void* d_Gx_freq,
+                                        const void* d_Gy_freq, int N, int W, int erosion, float dx, int B,
+                                        srk_stream_t stream, float* d_R);
+
 /* ---- storage-typed forms ----------------------------------------------------
  * Same operators with every image / cotangent / output buffer in the plan's
  * storage type (SRK_F32: float, SRK_F16: IEEE half, SRK_BF16: bfloat16),

@@ -68,6 +68,7 @@ _SIGS = {
     "srk_plan_set_schedule": [_P, _I],
     "srk_measure_cd": [_P, _I, _I, _I, _I, _P, _P, _P, _P],
     "srk_cd_after_shrinkage": [_P, _P, _I, _I, _I, _I, _F, _I, _I, _I, _P, _P, _P, _P],
+    "srk_training_forward_noalloc": [_P, _P, _P, _P, _I, _I, _I, _F, _I, _P, _P],
     "srk_autotune": [_I, _I, _I, _F, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)],
     "srk_plan_set_persistent": [_P, _I, _I, _I],
     "srk_plan_sync": [_P, _P],
