@@ -28,7 +28,7 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
     SRK_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     SRK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_persist<M, OP, T>, kThreads, sm2));
     if (per_sm < 1) return fail(SRK_ERR_UNSUPPORTED, "persistent kernel does not fit an SM (smem %zu)", sm2);
-    const int round = M / kWarps * 2 + (g.S + kWarps - 1) / kWarps;
+    const int round = M / lpu_of<M>() * 2 + (g.S + lpu_of<M>() - 1) / lpu_of<M>();
     int grid = nsm * per_sm;
     if (p->persist_grid > 0) grid = std::min(grid, p->persist_grid);
     // Tickets in flight ~ grid (x2 with prefetch): the lag between the phases
@@ -69,9 +69,10 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   int launches = 0;
   for (int w0 = 0; w0 < nwt; w0 += chunk) {
     const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
-    k_p1<M, OP, T><<<dim3(M / kWarps, c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
-    k_p2<M, OP><<<dim3(M / kWarps, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
-    k_p3<M, OP, T><<<dim3((g.S + kWarps - 1) / kWarps, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
+    constexpr int LPU = lpu_of<M>();
+    k_p1<M, OP, T><<<dim3(M / LPU, c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
+    k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
+    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
     launches += 3;
   }
   p->last_launches = launches;

@@ -37,7 +37,7 @@
 
 // CTAs per SM the kernels are compiled for (register cap 65536/(256*n)).
 #ifndef SRK_MIN_BLOCKS
-#define SRK_MIN_BLOCKS 3
+#define SRK_MIN_BLOCKS 4
 #endif
 
 namespace srk {
@@ -169,8 +169,9 @@ __device__ __forceinline__ float h_at(const OpArgs& a, int b, int k, int px, int
 // tile that crosses the bottom edge.
 template <int M, typename T>
 __device__ __forceinline__ void load_tile_column(const T* __restrict__ img, int N, const TileRef& t, int x, int lane,
-                                                 float (&v)[M / 32]) {
-  constexpr int EPT = M / 32;
+                                                 float (&v)[M / tpf_of<M>()]) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
   const int gx = t.x0 + x;
   if (!t.live || gx >= N) {
 #pragma unroll
@@ -181,22 +182,23 @@ __device__ __forceinline__ void load_tile_column(const T* __restrict__ img, int 
   const int rows = N - t.y0 - lane;  // rows available below this lane's first element
   if (N - t.y0 >= M) {
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) v[i] = ldf(col, 32 * i);
+    for (int i = 0; i < EPT; ++i) v[i] = ldf(col, TPF * i);
   } else {
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) v[i] = (32 * i < rows) ? ldf(col, 32 * i) : 0.f;
+    for (int i = 0; i < EPT; ++i) v[i] = (TPF * i < rows) ? ldf(col, TPF * i) : 0.f;
   }
 }
 
 template <int M, int OP, typename T>
 __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int w, int k, int x, int lane,
-                                            float2 (&z)[M / 32]) {
-  constexpr int EPT = M / 32;
+                                            float2 (&z)[M / tpf_of<M>()]) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
   if constexpr (OP == OP_ADJ) {
     const TileRef t0 = tile_of(g, 2 * w), t1 = tile_of(g, 2 * w + 1);
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
-      const int y = lane + 32 * i;
+      const int y = lane + TPF * i;
       const float re = h_at<T>(a, t0.b, k, t0.x0 + x, t0.y0 + y);
       const float im = t1.live ? h_at<T>(a, t1.b, k, t1.x0 + x, t1.y0 + y) : 0.f;
       z[i] = make_float2(re, im);
@@ -229,24 +231,26 @@ struct GradCol {
   int N;
   bool tested;
   int gx, gy0;
+  int st;  // row step between a thread's elements (threads per transform)
   __device__ __forceinline__ void at(int i, float& fx, float& fy) const {
     if (!tested) {
-      fx = (ldf(c + N, 32 * i) - ldf(c - N, 32 * i)) * 0.5f;
-      fy = (ldf(c + 1, 32 * i) - ldf(c - 1, 32 * i)) * 0.5f;
+      fx = (ldf(c + N, st * i) - ldf(c - N, st * i)) * 0.5f;
+      fy = (ldf(c + 1, st * i) - ldf(c - 1, st * i)) * 0.5f;
     } else {
-      const int gy = gy0 + 32 * i;
-      const float r = (gx + 1 < N) ? ldf(c + N, 32 * i) : 0.f;
-      const float l = (gx > 0) ? ldf(c - N, 32 * i) : 0.f;
-      const float d = (gy + 1 < N) ? ldf(c + 1, 32 * i) : 0.f;
-      const float u = (gy > 0) ? ldf(c - 1, 32 * i) : 0.f;
+      const int gy = gy0 + st * i;
+      const float r = (gx + 1 < N) ? ldf(c + N, st * i) : 0.f;
+      const float l = (gx > 0) ? ldf(c - N, st * i) : 0.f;
+      const float d = (gy + 1 < N) ? ldf(c + 1, st * i) : 0.f;
+      const float u = (gy > 0) ? ldf(c - 1, st * i) : 0.f;
       fx = (r - l) * 0.5f;
       fy = (d - u) * 0.5f;
     }
   }
 };
 template <typename T>
-__device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int gx, int gy0) {
+__device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int gx, int gy0, int st) {
   GradCol<T> gc;
+  gc.st = st;
   gc.c = f_img + (long long)gx * N + gy0;
   gc.N = N;
   gc.tested = e < 1;
@@ -260,8 +264,8 @@ template <int M>
 __device__ __forceinline__ unsigned valid_rows(const Geom& g, int y0, int lane) {
   unsigned m = 0;
 #pragma unroll
-  for (int i = 0; i < M / 32; ++i) {
-    const int y = lane + 32 * i;
+  for (int i = 0; i < M / tpf_of<M>(); ++i) {
+    const int y = lane + tpf_of<M>() * i;
     if (y >= g.e && y < g.e + g.S && y0 + y - g.e < g.Wout) m |= 1u << i;
   }
   return m;
@@ -269,8 +273,9 @@ __device__ __forceinline__ unsigned valid_rows(const Geom& g, int y0, int lane) 
 
 template <int M, int OP, typename T>
 __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, int w, int x, int lane,
-                                                float2 (&z0)[M / 32], float2 (&z1)[M / 32]) {
-  constexpr int EPT = M / 32;
+                                                float2 (&z0)[M / tpf_of<M>()], float2 (&z1)[M / tpf_of<M>()]) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
   const int N = a.N, W = a.W, e = a.e;
   if constexpr (OP == OP_FWD || OP == OP_VJP_F) {
 #pragma unroll
@@ -288,16 +293,16 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
         if (UX) {
 #pragma unroll
           for (int i = 0; i < EPT; ++i)
-            if (vm >> i & 1u) stf(UX, ob + 32 * i, h ? z0[i].y : z0[i].x);
+            if (vm >> i & 1u) stf(UX, ob + TPF * i, h ? z0[i].y : z0[i].x);
         }
         if (UY) {
 #pragma unroll
           for (int i = 0; i < EPT; ++i)
-            if (vm >> i & 1u) stf(UY, ob + 32 * i, h ? z1[i].y : z1[i].x);
+            if (vm >> i & 1u) stf(UY, ob + TPF * i, h ? z1[i].y : z1[i].x);
         }
         if (R) {
           const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e,
-                                         t.y0 + lane);
+                                         t.y0 + lane, TPF);
           // gradients for all rows first (every load in flight before the
           // first store); the result overwrites this image's half of z0
 #pragma unroll
@@ -309,7 +314,7 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
           }
 #pragma unroll
           for (int i = 0; i < EPT; ++i)
-            if (vm >> i & 1u) stf(R, ob + 32 * i, h ? z0[i].y : z0[i].x);
+            if (vm >> i & 1u) stf(R, ob + TPF * i, h ? z0[i].y : z0[i].x);
         }
       } else {  // OP_VJP_F: w = u * v
         const T* __restrict__ V = static_cast<const T*>(a.v);
@@ -317,12 +322,12 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
         float* __restrict__ WY = static_cast<float*>(a.out1);
         float v[EPT];
 #pragma unroll
-        for (int i = 0; i < EPT; ++i) v[i] = (vm >> i & 1u) ? ldf(V, ob + 32 * i) : 0.f;
+        for (int i = 0; i < EPT; ++i) v[i] = (vm >> i & 1u) ? ldf(V, ob + TPF * i) : 0.f;
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
           if (!(vm >> i & 1u)) continue;
-          WX[ob + 32 * i] = (h ? z0[i].y : z0[i].x) * v[i];
-          WY[ob + 32 * i] = (h ? z1[i].y : z1[i].x) * v[i];
+          WX[ob + TPF * i] = (h ? z0[i].y : z0[i].x) * v[i];
+          WY[ob + TPF * i] = (h ? z1[i].y : z1[i].x) * v[i];
         }
       }
     }
@@ -334,8 +339,8 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
     const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
     if constexpr (OP == OP_JVP) {
       // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52); re: conv of g, im: conv of dg
-      const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
-      const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane);
+      const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane, TPF);
+      const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane, TPF);
       T* __restrict__ DH = static_cast<T*>(a.out0);
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
@@ -348,7 +353,7 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
       }
 #pragma unroll
       for (int i = 0; i < EPT; ++i)
-        if (vm >> i & 1u) stf(DH, ob + 32 * i, z0[i].x);
+        if (vm >> i & 1u) stf(DH, ob + TPF * i, z0[i].x);
     } else {
       const T* __restrict__ LAM = static_cast<const T*>(a.v);
       const T* __restrict__ DLAM = static_cast<const T*>(a.dv);
@@ -357,9 +362,9 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
         if (!(vm >> i & 1u)) continue;
-        const float lam = ldf(LAM, ob + 32 * i), dlam = ldf(DLAM, ob + 32 * i);
-        WX[ob + 32 * i] = dlam * z0[i].x + lam * z0[i].y;
-        WY[ob + 32 * i] = dlam * z1[i].x + lam * z1[i].y;
+        const float lam = ldf(LAM, ob + TPF * i), dlam = ldf(DLAM, ob + TPF * i);
+        WX[ob + TPF * i] = dlam * z0[i].x + lam * z0[i].y;
+        WY[ob + TPF * i] = dlam * z1[i].x + lam * z1[i].y;
       }
     }
   } else {  // OP_ADJ: output is the full N x N image
@@ -373,27 +378,34 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
       T* __restrict__ O = static_cast<T*>(a.out0);
 #pragma unroll
       for (int i = 0; i < EPT; ++i)
-        if (vm >> i & 1u) stf(O, ob + 32 * i, h ? z0[i].y : z0[i].x);
+        if (vm >> i & 1u) stf(O, ob + TPF * i, h ? z0[i].y : z0[i].x);
     }
   }
 }
 
+// ---- unit geometry ----------------------------------------------------------------
+// A CTA of kWarps warps processes one unit of LPU lines (columns in P1/P3,
+// rows in P2); each line is one transform over TPF threads (line = thread /
+// TPF, t = thread % TPF, named barrier 1 + line when TPF > 32).
+template <int M>
+__host__ __device__ constexpr int lpu_of() { return kThreads / tpf_of<M>(); }
+
 // ---- staged gradients -------------------------------------------------------------
-// The 8 output columns of a P3 unit need the image columns gx-1 .. gx+8 and
-// rows gy-1 .. gy+S.  They are staged cooperatively (coalesced, every load
-// in flight) into shared memory: window column c <-> image column
-// x0 + e - 1 + c, window row r <-> image row y0 + e - 1 + r; out-of-image
-// elements are zero (the central-difference rule).
+// The LPU output columns of a P3 unit need the image columns gx-1 ..
+// gx+LPU and rows gy-1 .. gy+S.  They are staged cooperatively (coalesced,
+// every load in flight) into shared memory: window column c <-> image
+// column x0 + e - 1 + c, window row r <-> image row y0 + e - 1 + r;
+// out-of-image elements are zero (the central-difference rule).
 __host__ __device__ inline int gwin_pitch(int S) { return (S + 2 + 1) & ~1; }
-// 10 * gwin_pitch(S) floats <= 10 * (M + 3) <= 16 * (M + M/16 + 2): one
-// image's window always fits the 8 staging rows of the second field.
+// (LPU + 2) * gwin_pitch(S) floats <= (LPU + 2) * (M + 3) <= 2 * LPU * (M + M/16 + 2):
+// one image's window always fits the LPU staging rows of the second field.
 
 template <typename T>
 __device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int N, int gx0, int gy0, int S,
-                                                  float* __restrict__ dst) {
+                                                  int ncol, float* __restrict__ dst) {
   const int HP = gwin_pitch(S);
   const int H = S + 2;
-  for (int idx = threadIdx.x; idx < 10 * H; idx += kThreadsStage) {
+  for (int idx = threadIdx.x; idx < ncol * H; idx += kThreads) {
     const int c = idx / H, r = idx - (idx / H) * H;
     const int gx = gx0 + c, gy = gy0 + r;
     dst[c * HP + r] = (gx >= 0 && gx < N && gy >= 0 && gy < N) ? ldf(img, (long long)gx * N + gy) : 0.f;
@@ -401,26 +413,28 @@ __device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int
 }
 
 // Forward / tangent epilogue, round h, with the central differences read
-// from the staged window (window column warp+1 is this warp's image column).
-// FWD: round h finishes image h of the pair.  JVP: round 0 (window = f)
-// leaves the f terms in z0[i].y, round 1 (window = df) adds the df terms.
-// z0 stays stashed in the warp's row (z0s = its padded row, element i at
-// z0s[34 i]) to keep registers for the window reads.
+// from the staged window (window column line+1 is this line's image
+// column).  FWD: round h finishes image h of the pair.  JVP: round 0
+// (window = f) leaves the f terms in z0.y, round 1 (window = df) adds the df
+// terms.  z0 stays stashed in the line's padded row (z0s = row + t +
+// (t >> 4), element i at z0s[(TPF + TPF/16) i]) to keep registers free.
 template <int M, int OP, typename T>
-__device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, int w, int x, int warp, int lane,
-                                                int h, float2* __restrict__ z0s, const float2 (&z1)[M / 32],
+__device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, int w, int x, int line, int t, int h,
+                                                float2* __restrict__ z0s, const float2 (&z1)[M / tpf_of<M>()],
                                                 const float* __restrict__ win, int HP) {
-  constexpr int EPT = M / 32;
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
+  constexpr int RSP = TPF + TPF / 16;
   const int W = a.W;
-  const int rb = lane - g.e + 1;  // window row of element 0: y - e + 1, y = lane
-  const float* cm = win + warp * HP + rb;  // image column gx - 1
+  const int rb = t - g.e + 1;  // window row of element 0: y - e + 1, y = t
+  const float* cm = win + line * HP + rb;  // image column gx - 1
   const float* cc = cm + HP;               // gx
   const float* cp = cc + HP;               // gx + 1
-  const TileRef t = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
-  const int ox = t.x0 + x - g.e;
-  if (!t.live || ox >= g.Wout) return;
-  const unsigned vm = valid_rows<M>(g, t.y0, lane);
-  const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+  const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+  const int ox = tr.x0 + x - g.e;
+  if (!tr.live || ox >= g.Wout) return;
+  const unsigned vm = valid_rows<M>(g, tr.y0, t);
+  const long long ob = (long long)tr.b * W * W + (long long)ox * W + tr.y0 - g.e + t;
   if constexpr (OP == OP_FWD) {
     T* __restrict__ R = static_cast<T*>(a.out0);
     T* __restrict__ UX = static_cast<T*>(a.out_ux);
@@ -428,15 +442,15 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       if (!(vm >> i & 1u)) continue;
-      const float2 z0i = z0s[34 * i];
+      const float2 z0i = z0s[RSP * i];
       const float ux = h ? z0i.y : z0i.x;
       const float uy = h ? z1[i].y : z1[i].x;
-      if (UX) stf(UX, ob + 32 * i, ux);
-      if (UY) stf(UY, ob + 32 * i, uy);
+      if (UX) stf(UX, ob + TPF * i, ux);
+      if (UY) stf(UY, ob + TPF * i, uy);
       if (R) {
-        const float fx = (cp[32 * i] - cm[32 * i]) * 0.5f;
-        const float fy = (cc[32 * i + 1] - cc[32 * i - 1]) * 0.5f;
-        stf(R, ob + 32 * i, ux * fx + uy * fy);
+        const float fx = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
+        const float fy = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+        stf(R, ob + TPF * i, ux * fx + uy * fy);
       }
     }
   } else {
@@ -445,27 +459,26 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       if (!(vm >> i & 1u)) continue;
-      const float dx_ = (cp[32 * i] - cm[32 * i]) * 0.5f;
-      const float dy_ = (cc[32 * i + 1] - cc[32 * i - 1]) * 0.5f;
-      float2 z0i = z0s[34 * i];
+      const float dx_ = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
+      const float dy_ = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+      float2 z0i = z0s[RSP * i];
       if (h == 0) {
         z0i.y = z0i.y * dx_ + z1[i].y * dy_;
-        z0s[34 * i] = z0i;
+        z0s[RSP * i] = z0i;
       } else {
-        stf(static_cast<T*>(a.out0), ob + 32 * i, z0i.y + z0i.x * dx_ + z1[i].x * dy_);
+        stf(static_cast<T*>(a.out0), ob + TPF * i, z0i.y + z0i.x * dx_ + z1[i].x * dy_);
       }
     }
   }
 }
 
 // ---- phases ------------------------------------------------------------------
-
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int M) {
   for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
 }
 
-// Staging rows: stride RW + 2 float2 so that the 8 rows of a transposing
-// copy fall into different banks.
+// Staging rows: stride RW + 2 float2 so the rows of a transposing copy fall
+// into different banks.
 template <int M>
 __host__ __device__ constexpr int row_stride() { return fft_row_words(M) + 2; }
 // S2 rows are padded to a multiple of 8 columns (16-byte aligned float4 reads).
@@ -479,155 +492,165 @@ __host__ __device__ inline size_t wt_elems(int S) {
   return s1_elems<M, OP>() + (size_t)OpTraits<OP>::L * M * s2_pitch(S);
 }
 
-// Shared memory of every phase: the twiddle table and 2 x 8 staging rows.
+// Shared memory of every phase: the twiddle table and 2 x LPU staging rows.
 template <int M>
-constexpr size_t phase_smem_bytes() { return sizeof(float2) * (M + 2 * kWarps * row_stride<M>()); }
+constexpr size_t phase_smem_bytes() { return sizeof(float2) * (M + 2 * lpu_of<M>() * row_stride<M>()); }
 
-// Warp-wide copy between registers (strided order) and a padded row.
+// Copies between a thread's registers (strided order) and a padded row.
 template <int M>
-__device__ __forceinline__ void row_to_regs(const float2* __restrict__ row, float2 (&z)[M / 32], int lane) {
-  const float2* rd = row + lane + (lane >> 4);
+__device__ __forceinline__ void row_to_regs(const float2* __restrict__ row, float2 (&z)[M / tpf_of<M>()], int t) {
+  constexpr int TPF = tpf_of<M>();
+  const float2* rd = row + t + (t >> 4);
 #pragma unroll
-  for (int i = 0; i < M / 32; ++i) z[i] = rd[34 * i];
+  for (int i = 0; i < M / TPF; ++i) z[i] = rd[(TPF + TPF / 16) * i];
 }
 template <int M>
-__device__ __forceinline__ void regs_to_row(float2* __restrict__ row, const float2 (&z)[M / 32], int lane) {
-  float2* wr = row + lane + (lane >> 4);
+__device__ __forceinline__ void regs_to_row(float2* __restrict__ row, const float2 (&z)[M / tpf_of<M>()], int t) {
+  constexpr int TPF = tpf_of<M>();
+  float2* wr = row + t + (t >> 4);
 #pragma unroll
-  for (int i = 0; i < M / 32; ++i) wr[34 * i] = z[i];
+  for (int i = 0; i < M / TPF; ++i) wr[(TPF + TPF / 16) * i] = z[i];
 }
 
-// P1: warp `warp` transforms column x = xb*8 + warp of every field along y.
+// P1: line `line` transforms column x = xb*LPU + line of every field along y.
 template <int M, int OP, typename T>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
-                                       float2* __restrict__ row, const float2* __restrict__ tw, int warp, int lane) {
-  constexpr int EPT = M / 32;
+                                       float2* __restrict__ row, const float2* __restrict__ tw, int line, int t) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
   constexpr int K = OpTraits<OP>::K;
-  const int x = xb * kWarps + warp;
+  const int x = xb * lpu_of<M>() + line;
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
     float2 z[EPT];
-    load_column<M, OP, T>(a, g, w, k, x, lane, z);
-    fft<M, false>(z, row, tw, lane);
-    float2* dst = S1 + ((size_t)k * M + x) * M + lane;
+    load_column<M, OP, T>(a, g, w, k, x, t, z);
+    fft<M, false>(z, row, tw, t, 1 + line);
+    float2* dst = S1 + ((size_t)k * M + x) * M + t;
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) __stcg(dst + 32 * i, z[i]);
+    for (int i = 0; i < EPT; ++i) __stcg(dst + TPF * i, z[i]);
   }
 }
 
-// Transposing copy of an M x 8 block (M lines of 8 consecutive complex
-// values, line pitch `pitch`) into 8 staging rows of M values each.  All
-// threads of the CTA take part.
+// Transposing copy of an M x LPU block (M lines of LPU consecutive complex
+// values, line pitch `pitch`) into LPU staging rows of M values each.  All
+// threads of the CTA take part; every load is in flight before the
+// scattered shared stores.
 template <int M>
 __device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int pitch, float2* __restrict__ rows) {
   constexpr int RS = row_stride<M>();
-  constexpr int NIT = M * 4 / kThreads;  // float4 loads per thread
-  static_assert(M * 4 % kThreads == 0, "staging loop must divide evenly");
-  // all loads in flight first, then the scattered shared stores
+  constexpr int LPU = lpu_of<M>();
+  constexpr int Q = LPU / 2;                 // float4 per line
+  constexpr int NIT = M * Q / kThreads;      // float4 loads per thread
+  static_assert(M * Q % kThreads == 0, "staging loop must divide evenly");
   float4 q[NIT];
 #pragma unroll
   for (int j = 0; j < NIT; ++j) {
     const int idx = threadIdx.x + j * kThreads;
-    q[j] = __ldcg(reinterpret_cast<const float4*>(src + (size_t)(idx >> 2) * pitch + 2 * (idx & 3)));
+    q[j] = __ldcg(reinterpret_cast<const float4*>(src + (size_t)(idx / Q) * pitch + 2 * (idx % Q)));
   }
 #pragma unroll
   for (int j = 0; j < NIT; ++j) {
     const int idx = threadIdx.x + j * kThreads;
-    const int y = idx >> 2, cp = idx & 3;
+    const int y = idx / Q, cp = idx % Q;
     rows[(2 * cp) * RS + fft_pad(y)] = make_float2(q[j].x, q[j].y);
     rows[(2 * cp + 1) * RS + fft_pad(y)] = make_float2(q[j].z, q[j].w);
   }
 }
 
-// P2: rows ky0 .. ky0+7: FFT along x, spectral map, inverse, keep the valid
-// columns, write S2 rows.  All threads of the CTA take part.
+// P2: rows ky0 .. ky0+LPU-1: FFT along x, spectral map, inverse, keep the
+// valid columns, write S2 rows.  All threads of the CTA take part.
 template <int M, int OP>
 __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __restrict__ S2,
                                        const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
                                        const Geom& g, int ky0, float2* __restrict__ rows,
-                                       const float2* __restrict__ tw, int warp, int lane) {
-  constexpr int EPT = M / 32;
+                                       const float2* __restrict__ tw, int line, int t) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
+  constexpr int RSP = TPF + TPF / 16;
   constexpr int K = OpTraits<OP>::K;
   constexpr int RS = row_stride<M>();
+  constexpr int LPU = lpu_of<M>();
   const int S = g.S, e = g.e, P = s2_pitch(S);
-  // S1 viewed as rows ky (pitch M) of columns x: a transposing copy of the
-  // 8 columns ky0.. of the (x, ky) matrix -- i.e. S1[k][x][ky0 + c].
+  const int bar = 1 + line;
+  // S1[k][x][ky0 + c]: a transposing copy of LPU consecutive ky of every column x
 #pragma unroll
-  for (int k = 0; k < K; ++k) stage_rows<M>(S1 + (size_t)k * M * M + ky0, M, rows + k * kWarps * RS);
+  for (int k = 0; k < K; ++k) stage_rows<M>(S1 + (size_t)k * M * M + ky0, M, rows + k * LPU * RS);
   __syncthreads();
-  const int ky = ky0 + warp;
-  float2* row0 = rows + warp * RS;              // field 0 / exchange
-  float2* row1 = rows + (kWarps + warp) * RS;   // field 1 or the stash
-  const float2* gxr = Gx + (size_t)ky * M + lane;
-  const float2* gyr = Gy + (size_t)ky * M + lane;
+  const int ky = ky0 + line;
+  float2* row0 = rows + line * RS;           // field 0 / exchange
+  float2* row1 = rows + (LPU + line) * RS;   // field 1 or the stash
+  const float2* gxr = Gx + (size_t)ky * M + t;
+  const float2* gyr = Gy + (size_t)ky * M + t;
   auto spec = [&](float2 z, float2 G) { return conjG ? cmulc(z, G) : cmul(z, G); };
   auto emit = [&](const float2 (&o)[EPT], int l) {
-    float2* dst = S2 + ((size_t)l * M + ky) * P - e + lane;
+    float2* dst = S2 + ((size_t)l * M + ky) * P - e + t;
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
-      const int xv = lane + 32 * i - e;
-      if (xv >= 0 && xv < S) __stcg(dst + 32 * i, o[i]);
+      const int xv = t + TPF * i - e;
+      if (xv >= 0 && xv < S) __stcg(dst + TPF * i, o[i]);
     }
   };
   float2 z[EPT];
-  row_to_regs<M>(row0, z, lane);
-  fft<M, false>(z, row0, tw, lane);
+  row_to_regs<M>(row0, z, t);
+  fft<M, false>(z, row0, tw, t, bar);
   if constexpr (K == 1) {
-    regs_to_row<M>(row1, z, lane);  // stash Z(ky, .)
+    regs_to_row<M>(row1, z, t);  // stash Z(ky, .): each thread rereads only its own elements
 #pragma unroll
     for (int l = 0; l < 2; ++l) {
       const float2* gr = l ? gyr : gxr;
-      const float2* st = row1 + lane + (lane >> 4);
+      const float2* st = row1 + t + (t >> 4);
 #pragma unroll
-      for (int i = 0; i < EPT; ++i) z[i] = spec(st[34 * i], __ldg(gr + 32 * i));
-      fft<M, true>(z, row0, tw, lane);
-      emit(z, 0 + l);
+      for (int i = 0; i < EPT; ++i) z[i] = spec(st[RSP * i], __ldg(gr + TPF * i));
+      fft<M, true>(z, row0, tw, t, bar);
+      emit(z, l);
     }
   } else {
-    __syncwarp();
-    regs_to_row<M>(row0, z, lane);  // stash Z0(ky, .) in its own row
-    row_to_regs<M>(row1, z, lane);
-    fft<M, false>(z, row1, tw, lane);
-    const float2* st = row0 + lane + (lane >> 4);
+    group_sync<TPF>(bar);
+    regs_to_row<M>(row0, z, t);  // stash Z0(ky, .) in its own row
+    row_to_regs<M>(row1, z, t);
+    fft<M, false>(z, row1, tw, t, bar);
+    const float2* st = row0 + t + (t >> 4);
 #pragma unroll
     for (int i = 0; i < EPT; ++i)
-      z[i] = cadd(spec(st[34 * i], __ldg(gxr + 32 * i)), spec(z[i], __ldg(gyr + 32 * i)));
-    fft<M, true>(z, row1, tw, lane);
+      z[i] = cadd(spec(st[RSP * i], __ldg(gxr + TPF * i)), spec(z[i], __ldg(gyr + TPF * i)));
+    fft<M, true>(z, row1, tw, t, bar);
     emit(z, 0);
   }
 }
 
-// P3: columns x' = xb*8 .. +7: stage them, inverse FFT along ky, epilogue.
-// All threads of the CTA take part (warps without a valid column still join
-// the barriers).  For the forward and tangent epilogues with erosion >= 1
-// the image columns the central differences need are staged in shared
-// memory after the transforms, in the rows the transforms no longer use.
+// P3: columns x' = xb*LPU .. +LPU-1: stage them, inverse FFT along ky,
+// epilogue.  All threads of the CTA take part (lines without a valid column
+// still join the barriers).  For the forward and tangent epilogues with
+// erosion >= 1 the image columns the central differences need are staged in
+// shared memory after the transforms, in the rows they no longer use.
 template <int M, int OP, typename T>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
-                                       float2* __restrict__ rows, const float2* __restrict__ tw, int warp,
-                                       int lane) {
-  constexpr int EPT = M / 32;
+                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
   constexpr int L = OpTraits<OP>::L;
   constexpr int RS = row_stride<M>();
+  constexpr int LPU = lpu_of<M>();
   constexpr bool GRAD = (OP == OP_FWD || OP == OP_JVP);
   const int P = s2_pitch(g.S);
-  const int x0 = xb * kWarps;
+  const int x0 = xb * LPU;
+  const int bar = 1 + line;
 #pragma unroll
-  for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * kWarps * RS);
+  for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
   __syncthreads();
-  const int xv = x0 + warp;
+  const int xv = x0 + line;
   const bool active = xv < g.S;
-  float2* row0 = rows + warp * RS;
-  float2* row1 = rows + (kWarps + warp) * RS;
+  float2* row0 = rows + line * RS;
+  float2* row1 = rows + (LPU + line) * RS;
   float2 z0[EPT], z1[EPT];
   if (active) {
-    row_to_regs<M>(row0, z0, lane);
-    fft<M, true>(z0, row0, tw, lane);
+    row_to_regs<M>(row0, z0, t);
+    fft<M, true>(z0, row0, tw, t, bar);
     if constexpr (L == 2) {
-      __syncwarp();
-      regs_to_row<M>(row0, z0, lane);   // stash, reload after the second transform
-      row_to_regs<M>(row1, z1, lane);
-      fft<M, true>(z1, row1, tw, lane);
+      group_sync<TPF>(bar);
+      regs_to_row<M>(row0, z0, t);   // stash, reread after the second transform
+      row_to_regs<M>(row1, z1, t);
+      fft<M, true>(z1, row1, tw, t, bar);
     }
   }
   if constexpr (L == 1) {
@@ -636,29 +659,30 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   }
   if constexpr (GRAD) {
     if (a.e >= 1) {
-      // two rounds, one image window each, in the row1 block
-      float* win = reinterpret_cast<float*>(rows + kWarps * RS);
+      // two rounds, one image window each, in the second field's rows
+      float* win = reinterpret_cast<float*>(rows + LPU * RS);
       const int HP = gwin_pitch(g.S);
-      float2* z0s = row0 + lane + (lane >> 4);
+      float2* z0s = row0 + t + (t >> 4);
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
-        __syncthreads();  // row1 no longer used (round 0) / window consumed (round 1)
-        const TileRef t = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+        __syncthreads();  // rows of field 1 no longer used (round 0) / window consumed (round 1)
+        const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
         const T* img = static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI);
-        if (t.live)
-          stage_grad_window<T>(img + (long long)t.b * a.N * a.N, a.N, t.x0 + x0 + a.e - 1, t.y0 + a.e - 1, g.S, win);
+        if (tr.live)
+          stage_grad_window<T>(img + (long long)tr.b * a.N * a.N, a.N, tr.x0 + x0 + a.e - 1, tr.y0 + a.e - 1, g.S,
+                               LPU + 2, win);
         __syncthreads();
-        if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, warp, lane, h, z0s, z1, win, HP);
+        if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, h, z0s, z1, win, HP);
       }
       return;
     }
   }
   if (!active) return;
   if constexpr (L == 2) {
-    __syncwarp();
-    row_to_regs<M>(row0, z0, lane);
+    group_sync<TPF>(bar);
+    row_to_regs<M>(row0, z0, t);
   }
-  epilogue_column<M, OP, T>(a, g, w, xv + g.e, lane, z0, z1);
+  epilogue_column<M, OP, T>(a, g, w, xv + g.e, t, z0, z1);
 }
 
 // ---- three-launch schedule (one kernel per phase over a chunk of WTs) ------
@@ -666,12 +690,13 @@ template <int M, int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
   extern __shared__ float2 sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int TPF = tpf_of<M>();
+  const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
   load_twiddles(sm, twg, M);
   __syncthreads();
   const int wl = blockIdx.y;
-  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + warp * row_stride<M>(),
-                   sm, warp, lane);
+  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + line * row_stride<M>(),
+                   sm, line, t);
 }
 
 template <int M, int OP>
@@ -679,21 +704,23 @@ __global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG, Geom g,
      const float2* __restrict__ twg) {
   extern __shared__ float2 sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int TPF = tpf_of<M>();
+  const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
   load_twiddles(sm, twg, M);
   float2* base = scratch + blockIdx.y * wt_elems<M, OP>(g.S);
-  phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, blockIdx.x * kWarps, sm + M, sm, warp, lane);
+  phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, blockIdx.x * lpu_of<M>(), sm + M, sm, line, t);
 }
 
 template <int M, int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
 k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
   extern __shared__ float2 sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int TPF = tpf_of<M>();
+  const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
   load_twiddles(sm, twg, M);
   const int wl = blockIdx.y;
   phase3<M, OP, T>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x, sm + M, sm,
-                   warp, lane);
+                   line, t);
 }
 
 // ---- persistent schedule ---------------------------------------------------------
@@ -761,8 +788,10 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
           const float2* __restrict__ twg, float2* __restrict__ scratch, int nwt, Ctl* ctl, PersistParams pp) {
   extern __shared__ float2 sm[];
   __shared__ int s_t[2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n1 = M / kWarps, n2 = M / kWarps, n3 = (g.S + kWarps - 1) / kWarps;
+  constexpr int TPF = tpf_of<M>();
+  constexpr int LPU = lpu_of<M>();
+  const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
+  const int n1 = M / LPU, n2 = M / LPU, n3 = (g.S + LPU - 1) / LPU;
   const int round = n1 + n2 + n3;
   const int lag = pp.lag, nslot = pp.nslot;
   const long long total = (long long)(nwt + 2 * lag) * round;
@@ -800,11 +829,11 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
     if (live) {
       float2* base = scratch + (size_t)slot * slot_elems;
       if (phase == 1) {
-        phase1<M, OP, T>(a, g, w, unit, base, buf + warp * row_stride<M>(), tw, warp, lane);
+        phase1<M, OP, T>(a, g, w, unit, base, buf + line * row_stride<M>(), tw, line, t);
       } else if (phase == 2) {
-        phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * kWarps, buf, tw, warp, lane);
+        phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * LPU, buf, tw, line, t);
       } else {
-        phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf, tw, warp, lane);
+        phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf, tw, line, t);
       }
     }
     __syncthreads();  // every thread's scratch stores of this unit are issued

@@ -1,10 +1,10 @@
-// fft_warp.cuh — one-warp complex FFT of length M (128..1024) for sm_100a.
+// fft_warp.cuh — complex FFT of length M (128..512) by one warp or a warp pair, sm_100a.
 //
-// Layout contract (both directions):
-//   lane t holds x[i] = X[t + 32*i], i in [0, M/32)      ("strided" order)
-// so a warp loads/stores one contiguous column of M complex values with
-// fully coalesced 256-byte requests, and the transform result comes back in
-// the same order (natural frequency order, no bit reversal).
+// Layout contract (both directions): the TPF threads of a transform (a warp,
+// or a pair of warps for M = 512) hold x[i] = X[t + TPF*i], i < M/TPF
+// ("strided" order), so each warp loads/stores one contiguous column with
+// fully coalesced requests, and the result comes back in the same order
+// (natural frequency order, no bit reversal).
 //
 // Algorithm: Stockham auto-sort, one radix-R pass per stage (mixed radix,
 // R in {2,4,8,16}).  Pass p with span Ns (product of the previous radices)
@@ -99,46 +99,58 @@ struct Dft<2, INV> {
   }
 };
 
-// Per-lane part P(lane) and compile-time part C(b, r) of the write index
-// (j/NS)*NS*R + (j mod NS) + r*NS of butterfly j = lane + 32*b.
-template <int R, int NS>
-__host__ __device__ constexpr int pass_P(int lane) {
-  return NS >= 32 ? lane : (lane / NS) * NS * R + (lane % NS);
+// Per-thread part P(t) and compile-time part C(b, r) of the write index
+// (j/NS)*NS*R + (j mod NS) + r*NS of butterfly j = t + TPF*b, where TPF is
+// the number of threads that share one transform (32 or 64).
+template <int R, int NS, int TPF>
+__host__ __device__ constexpr int pass_P(int t) {
+  return NS >= TPF ? t : (t / NS) * NS * R + (t % NS);
 }
-template <int R, int NS>
+template <int R, int NS, int TPF>
 __host__ __device__ constexpr int pass_C(int b, int r) {
-  return NS >= 32 ? ((32 * b) / NS) * NS * R + (32 * b) % NS + r * NS : 32 * b * R + r * NS;
+  return NS >= TPF ? ((TPF * b) / NS) * NS * R + (TPF * b) % NS + r * NS : TPF * b * R + r * NS;
 }
-// fft_pad(P + C) == fft_pad(P) + fft_pad(C) for every lane, butterfly and
-// leg: then every shared-memory write is (per-lane base) + (immediate).
-template <int M, int R, int NS>
+// fft_pad(P + C) == fft_pad(P) + fft_pad(C) for every thread, butterfly and
+// leg: then every shared-memory write is (per-thread base) + (immediate).
+template <int M, int R, int NS, int TPF>
 __host__ __device__ constexpr bool pad_separable() {
-  for (int lane = 0; lane < 32; ++lane)
-    for (int b = 0; b < M / 32 / R; ++b)
+  for (int t = 0; t < TPF; ++t)
+    for (int b = 0; b < M / TPF / R; ++b)
       for (int r = 0; r < R; ++r) {
-        const int P = pass_P<R, NS>(lane), C = pass_C<R, NS>(b, r);
+        const int P = pass_P<R, NS, TPF>(t), C = pass_C<R, NS, TPF>(b, r);
         if (fft_pad(P + C) != fft_pad(P) + fft_pad(C)) return false;
       }
   return true;
 }
 
-// One Stockham pass.  sm: this warp's padded exchange row; tw: W_M table.
-template <int M, int R, int NS, bool FIRST, bool LAST, bool INV>
-__device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict__ sm,
-                                         const float2* __restrict__ tw, int lane) {
-  constexpr int EPT = M / 32;
-  constexpr int NB = EPT / R;
-  static_assert(EPT % R == 0, "radix must divide elements per lane");
-  static_assert(LAST || pad_separable<M, R, NS>(), "padded write index must split into base + immediate");
-  if constexpr (!FIRST) {
-    // fft_pad(lane + 32 i) = lane + (lane >> 4) + 34 i
-    const float2* rd = sm + lane + (lane >> 4);
-#pragma unroll
-    for (int i = 0; i < EPT; ++i) x[i] = rd[34 * i];
+// Barrier over the threads of one transform: the warp itself, or a named
+// barrier (id >= 1) over the TPF threads of a multi-warp group.
+template <int TPF>
+__device__ __forceinline__ void group_sync(int bar) {
+  if constexpr (TPF == 32) {
     __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(TPF) : "memory");
+  }
+}
+
+// One Stockham pass.  sm: this transform's padded exchange row; tw: W_M table.
+template <int M, int TPF, int R, int NS, bool FIRST, bool LAST, bool INV>
+__device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restrict__ sm,
+                                         const float2* __restrict__ tw, int t, int bar) {
+  constexpr int EPT = M / TPF;
+  constexpr int NB = EPT / R;
+  static_assert(EPT % R == 0, "radix must divide elements per thread");
+  static_assert(LAST || pad_separable<M, R, NS, TPF>(), "padded write index must split into base + immediate");
+  if constexpr (!FIRST) {
+    // fft_pad(t + TPF i) = t + (t >> 4) + (TPF + TPF/16) i
+    const float2* rd = sm + t + (t >> 4);
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) x[i] = rd[(TPF + TPF / 16) * i];
+    group_sync<TPF>(bar);
   }
   float2* wr = nullptr;
-  if constexpr (!LAST) wr = sm + fft_pad(pass_P<R, NS>(lane));
+  if constexpr (!LAST) wr = sm + fft_pad(pass_P<R, NS, TPF>(t));
   // twiddle exponent step: W_{NS*R}^{r k} = W_M^{r k (M/(NS R))}
   constexpr int TS = M / (NS * R);
 #pragma unroll
@@ -147,8 +159,8 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict
 #pragma unroll
     for (int r = 0; r < R; ++r) a[r] = x[b + r * NB];
     if constexpr (!FIRST) {
-      // k = (lane + 32 b) mod NS
-      const int k = (NS <= 32) ? (lane & (NS - 1)) : (lane + ((32 * b) & (NS - 1)));
+      // k = (t + TPF b) mod NS
+      const int k = (NS <= TPF) ? (t & (NS - 1)) : (t + ((TPF * b) & (NS - 1)));
 #pragma unroll
       for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], tw[r * k * TS]);
     }
@@ -158,36 +170,39 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / 32], float2* __restrict
       for (int r = 0; r < R; ++r) x[b + r * NB] = a[r];
     } else {
 #pragma unroll
-      for (int r = 0; r < R; ++r) wr[fft_pad(pass_C<R, NS>(b, r))] = a[r];
+      for (int r = 0; r < R; ++r) wr[fft_pad(pass_C<R, NS, TPF>(b, r))] = a[r];
     }
   }
-  if constexpr (!LAST) __syncwarp();
+  if constexpr (!LAST) group_sync<TPF>(bar);
 }
 
-// Full transform.  All 32 lanes of the warp must call it together.
-template <int M, bool INV>
-__device__ __forceinline__ void fft(float2 (&x)[M / 32], float2* __restrict__ sm,
-                                    const float2* __restrict__ tw, int lane) {
-  __syncwarp();  // the row may still be read by lanes finishing a previous use
+// Threads per transform: a warp for M <= 256, a 64-thread pair of warps for
+// M = 512 (8 values per thread keeps registers low enough for 5 CTAs/SM).
+template <int M>
+__host__ __device__ constexpr int tpf_of() { return M >= 512 ? 64 : 32; }
+
+// Full transform over the TPF threads of a group; t = thread index in the
+// group, bar = its named barrier (ignored for TPF = 32).  Data layout:
+// thread t holds X[t + TPF*i].
+template <int M, bool INV, int TPF = tpf_of<M>()>
+__device__ __forceinline__ void fft(float2 (&x)[M / TPF], float2* __restrict__ sm, const float2* __restrict__ tw,
+                                    int t, int bar) {
+  group_sync<TPF>(bar);  // the row may still be read by threads finishing a previous use
   if constexpr (M == 128) {
-    fft_pass<M, 4, 1, true, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 4, 4, false, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 4, 16, false, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 2, 64, false, true, INV>(x, sm, tw, lane);
+    fft_pass<M, TPF, 4, 1, true, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 4, 4, false, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 4, 16, false, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 2, 64, false, true, INV>(x, sm, tw, t, bar);
   } else if constexpr (M == 256) {
-    fft_pass<M, 8, 1, true, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 8, 8, false, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 4, 64, false, true, INV>(x, sm, tw, lane);
+    fft_pass<M, TPF, 8, 1, true, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 8, 8, false, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 4, 64, false, true, INV>(x, sm, tw, t, bar);
   } else if constexpr (M == 512) {
-    fft_pass<M, 8, 1, true, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 8, 8, false, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 8, 64, false, true, INV>(x, sm, tw, lane);
-  } else if constexpr (M == 1024) {
-    fft_pass<M, 16, 1, true, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 8, 16, false, false, INV>(x, sm, tw, lane);
-    fft_pass<M, 8, 128, false, true, INV>(x, sm, tw, lane);
+    fft_pass<M, TPF, 8, 1, true, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 8, 8, false, false, INV>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, 8, 64, false, true, INV>(x, sm, tw, t, bar);
   } else {
-    static_assert(M == 128 || M == 256 || M == 512 || M == 1024, "unsupported FFT length");
+    static_assert(M == 128 || M == 256 || M == 512, "unsupported FFT length");
   }
 }
 
