@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass"],
                    help="override the autotuned kernel schedule (profiling)")
+    p.add_argument("--tile-M", type=int, default=0,
+                   help="fixed tile size instead of the autotuned one (profiling: no tuner launches)")
     return p.parse_args()
 
 
@@ -266,7 +268,7 @@ def run_ours(a):
     _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
     E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17)
     R = torch.empty((B, W, W), device="cuda")
-    plan = srk.SrkPlan(N, W, e, dx, B, tile_M=srk.SRK_TILE_AUTOTUNE)
+    plan = srk.SrkPlan(N, W, e, dx, B, tile_M=a.tile_M if a.tile_M else srk.SRK_TILE_AUTOTUNE)
     if a.schedule != "auto":
         plan.set_schedule(srk.SRK_SCHEDULE_PERSISTENT if a.schedule == "persistent" else srk.SRK_SCHEDULE_THREE_PASS)
     step = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)

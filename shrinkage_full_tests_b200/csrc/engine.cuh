@@ -33,6 +33,7 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <cstdint>
+#include <type_traits>
 #include "fft_warp.cuh"
 
 // CTAs per SM the kernels are compiled for (register cap 65536/(256*n)).
@@ -405,11 +406,48 @@ __device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int
                                                   int ncol, float* __restrict__ dst) {
   const int HP = gwin_pitch(S);
   const int H = S + 2;
-  for (int idx = threadIdx.x; idx < ncol * H; idx += kThreads) {
-    const int c = idx / H, r = idx - (idx / H) * H;
+  // (c, r) of element threadIdx.x + j*kThreads, advanced without division
+  const int dc = kThreads / H, dr = kThreads - dc * H;
+  int c = threadIdx.x / H, r = threadIdx.x - c * H;
+  for (; c < ncol; c += dc, r += dr) {
+    if (r >= H) { r -= H; ++c; if (c >= ncol) break; }
     const int gx = gx0 + c, gy = gy0 + r;
     dst[c * HP + r] = (gx >= 0 && gx < N && gy >= 0 && gy < N) ? ldf(img, (long long)gx * N + gy) : 0.f;
   }
+}
+
+// The same window copied with asynchronous 4-byte global->shared copies
+// (cp.async, zero fill outside the image): the caller commits the group and
+// waits for it later, so the loads overlap other work.  FP32 images only.
+__device__ __forceinline__ void cp_async4_zfill(float* dst, const float* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ void stage_grad_window_async(const float* __restrict__ img, int N, int gx0, int gy0, int S,
+                                                        int ncol, float* __restrict__ dst) {
+  const int HP = gwin_pitch(S);
+  const int H = S + 2;
+  const int dc = kThreads / H, dr = kThreads - dc * H;
+  int c = threadIdx.x / H, r = threadIdx.x - c * H;
+  for (; c < ncol; c += dc, r += dr) {
+    if (r >= H) { r -= H; ++c; if (c >= ncol) break; }
+    const int gx = gx0 + c, gy = gy0 + r;
+    const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
+    cp_async4_zfill(dst + c * HP + r, in ? img + (long long)gx * N + gy : img, in);
+  }
+}
+// Floats of one staged window at tile size M (S <= M - 2 when erosion >= 1).
+template <int M>
+__host__ __device__ constexpr int p3_window_floats() { return (lpu_of<M>() + 2) * M; }
+// P3 of the three-launch schedule prefetches the first window asynchronously
+// into a buffer of its own (forward / tangent epilogues on FP32 images).
+template <int OP, typename T>
+__host__ __device__ constexpr bool p3_async_window() {
+  return (OP == OP_FWD || OP == OP_JVP) && std::is_same<T, float>::value;
 }
 
 // Forward / tangent epilogue, round h, with the central differences read
@@ -474,7 +512,7 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
 
 // ---- phases ------------------------------------------------------------------
 __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restrict__ twg, int M) {
-  for (int i = threadIdx.x; i < M; i += blockDim.x) tw[i] = twg[i];
+  for (int i = threadIdx.x; i < tw_entries(M); i += blockDim.x) tw[i] = twg[i];
 }
 
 // Staging rows: stride RW + 2 float2 so the rows of a transposing copy fall
@@ -623,18 +661,34 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
 // still join the barriers).  For the forward and tangent epilogues with
 // erosion >= 1 the image columns the central differences need are staged in
 // shared memory after the transforms, in the rows they no longer use.
-template <int M, int OP, typename T>
+template <int M, int OP, typename T, bool ASYNC = false>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
-                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t) {
+                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
+                                       float* __restrict__ win0 = nullptr) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int L = OpTraits<OP>::L;
   constexpr int RS = row_stride<M>();
   constexpr int LPU = lpu_of<M>();
   constexpr bool GRAD = (OP == OP_FWD || OP == OP_JVP);
+  static_assert(!ASYNC || p3_async_window<OP, T>(), "asynchronous window only for FP32 forward / tangent");
   const int P = s2_pitch(g.S);
   const int x0 = xb * LPU;
   const int bar = 1 + line;
+  // window h: image (pair member h, or f / df) columns x0+e-1 .. x0+e+LPU, rows y0+e-1 .. y0+e+S
+  auto issue_window = [&](int h, float* dst) {
+    if constexpr (ASYNC) {
+      const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+      const float* img = static_cast<const float*>(OP == OP_FWD || h == 0 ? a.I : a.dI);
+      if (tr.live)
+        stage_grad_window_async(img + (long long)tr.b * a.N * a.N, a.N, tr.x0 + x0 + a.e - 1, tr.y0 + a.e - 1, g.S,
+                                LPU + 2, dst);
+      cp_async_commit();
+    }
+  };
+  if constexpr (ASYNC) {
+    if (a.e >= 1) issue_window(0, win0);  // in flight during the staging and the transforms
+  }
 #pragma unroll
   for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
   __syncthreads();
@@ -656,6 +710,24 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   if constexpr (L == 1) {
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z1[i] = make_float2(0.f, 0.f);
+  }
+  if constexpr (ASYNC) {
+    if (a.e >= 1) {
+      // window 0 has been arriving in its own buffer; window 1 goes to the
+      // second field's rows once every line is done with them
+      float* win1 = reinterpret_cast<float*>(rows + LPU * RS);
+      const int HP = gwin_pitch(g.S);
+      float2* z0s = row0 + t + (t >> 4);
+      __syncthreads();
+      issue_window(1, win1);
+      cp_async_wait<1>();
+      __syncthreads();
+      if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, 0, z0s, z1, win0, HP);
+      cp_async_wait<0>();
+      __syncthreads();
+      if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, 1, z0s, z1, win1, HP);
+      return;
+    }
   }
   if constexpr (GRAD) {
     if (a.e >= 1) {
@@ -719,8 +791,10 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
   const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
   load_twiddles(sm, twg, M);
   const int wl = blockIdx.y;
-  phase3<M, OP, T>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x, sm + M, sm,
-                   line, t);
+  constexpr bool ASYNC = p3_async_window<OP, T>();
+  float* win0 = ASYNC ? reinterpret_cast<float*>(sm + M + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
+  phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
+                          sm + M, sm, line, t, win0);
 }
 
 // ---- persistent schedule ---------------------------------------------------------

@@ -17,8 +17,8 @@
 // M + M/16 float2 (one pad word per 16, which makes the scatter of the
 // first pass bank-conflict free).
 //
-// Twiddles W_M^m = exp(-2*pi*i*m/M) come from a table in shared memory that
-// the host fills from double-precision cos/sin (rounded once to float);
+// Twiddles come from a table in shared memory, one block per pass
+// (tw_entry), filled from double-precision cos/sin rounded once to float;
 // the inverse transform uses their conjugates.  The transforms are
 // unnormalised in both directions.
 #pragma once
@@ -99,6 +99,58 @@ struct Dft<2, INV> {
   }
 };
 
+// ---- radix schedule and twiddle-table layout ---------------------------------
+// Passes of the M-point transform: (radix R, span NS before the pass).
+struct PassDesc { int R, NS; };
+__host__ __device__ constexpr int fft_npasses(int M) { return M == 128 ? 4 : 3; }
+__host__ __device__ constexpr PassDesc fft_pass_desc(int M, int p) {
+  return M == 128   ? (p == 0 ? PassDesc{4, 1} : p == 1 ? PassDesc{4, 4} : p == 2 ? PassDesc{4, 16} : PassDesc{2, 64})
+         : M == 256 ? (p == 0 ? PassDesc{8, 1} : p == 1 ? PassDesc{8, 8} : PassDesc{4, 64})
+                    : (p == 0 ? PassDesc{8, 1} : p == 1 ? PassDesc{8, 8} : PassDesc{8, 64});
+}
+// The twiddle table holds, for every pass p >= 1, the NS entries
+// W_{NS R}^k = exp(-2 pi i k / (NS R)), k < NS, one block per pass; a thread
+// reads the one entry of its butterfly (consecutive threads read consecutive
+// k or the same word: no bank conflicts) and forms the powers W^{r k},
+// r < R, by complex products (tw_powers).
+__host__ __device__ constexpr int tw_offset(int M, int p) {
+  int off = 0;
+  for (int q = 1; q < p; ++q) off += fft_pass_desc(M, q).NS;
+  return off;
+}
+__host__ __device__ constexpr int tw_entries(int M) { return tw_offset(M, fft_npasses(M)); }
+// Exponent of table entry idx as the fraction num/den of a full turn.
+__host__ __device__ inline void tw_entry(int M, int idx, int& num, int& den) {
+  for (int p = 1; p < fft_npasses(M); ++p) {
+    const PassDesc d = fft_pass_desc(M, p);
+    if (idx < d.NS) {
+      num = idx;
+      den = d.NS * d.R;
+      return;
+    }
+    idx -= d.NS;
+  }
+  num = 0;
+  den = 1;
+}
+
+// w[r] = w1^r for 1 <= r < R, by at most three dependent products (w[0] is
+// not set): the rounding error stays within a few units of the last place.
+template <int R>
+__device__ __forceinline__ void tw_powers(float2 w1, float2 (&w)[R]) {
+  w[1] = w1;
+  if constexpr (R >= 4) {
+    w[2] = cmul(w1, w1);
+    w[3] = cmul(w[2], w1);
+  }
+  if constexpr (R == 8) {
+    w[4] = cmul(w[2], w[2]);
+    w[5] = cmul(w[4], w1);
+    w[6] = cmul(w[4], w[2]);
+    w[7] = cmul(w[4], w[3]);
+  }
+}
+
 // Per-thread part P(t) and compile-time part C(b, r) of the write index
 // (j/NS)*NS*R + (j mod NS) + r*NS of butterfly j = t + TPF*b, where TPF is
 // the number of threads that share one transform (32 or 64).
@@ -135,7 +187,7 @@ __device__ __forceinline__ void group_sync(int bar) {
 }
 
 // One Stockham pass.  sm: this transform's padded exchange row; tw: W_M table.
-template <int M, int TPF, int R, int NS, bool FIRST, bool LAST, bool INV>
+template <int M, int TPF, int R, int NS, bool FIRST, bool LAST, bool INV, int TWOFF>
 __device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restrict__ sm,
                                          const float2* __restrict__ tw, int t, int bar) {
   constexpr int EPT = M / TPF;
@@ -151,8 +203,7 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restric
   }
   float2* wr = nullptr;
   if constexpr (!LAST) wr = sm + fft_pad(pass_P<R, NS, TPF>(t));
-  // twiddle exponent step: W_{NS*R}^{r k} = W_M^{r k (M/(NS R))}
-  constexpr int TS = M / (NS * R);
+  const float2* twp = tw + TWOFF;  // this pass's W_{NS R}^k block
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     float2 a[R];
@@ -161,8 +212,10 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restric
     if constexpr (!FIRST) {
       // k = (t + TPF b) mod NS
       const int k = (NS <= TPF) ? (t & (NS - 1)) : (t + ((TPF * b) & (NS - 1)));
+      float2 w[R];
+      tw_powers<R>(twp[k], w);
 #pragma unroll
-      for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], tw[r * k * TS]);
+      for (int r = 1; r < R; ++r) a[r] = twmul<INV>(a[r], w[r]);
     }
     Dft<R, INV>::run(a);
     if constexpr (LAST) {
@@ -188,21 +241,15 @@ template <int M, bool INV, int TPF = tpf_of<M>()>
 __device__ __forceinline__ void fft(float2 (&x)[M / TPF], float2* __restrict__ sm, const float2* __restrict__ tw,
                                     int t, int bar) {
   group_sync<TPF>(bar);  // the row may still be read by threads finishing a previous use
-  if constexpr (M == 128) {
-    fft_pass<M, TPF, 4, 1, true, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 4, 4, false, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 4, 16, false, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 2, 64, false, true, INV>(x, sm, tw, t, bar);
-  } else if constexpr (M == 256) {
-    fft_pass<M, TPF, 8, 1, true, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 8, 8, false, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 4, 64, false, true, INV>(x, sm, tw, t, bar);
-  } else if constexpr (M == 512) {
-    fft_pass<M, TPF, 8, 1, true, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 8, 8, false, false, INV>(x, sm, tw, t, bar);
-    fft_pass<M, TPF, 8, 64, false, true, INV>(x, sm, tw, t, bar);
-  } else {
-    static_assert(M == 128 || M == 256 || M == 512, "unsupported FFT length");
+  static_assert(M == 128 || M == 256 || M == 512, "unsupported FFT length");
+  constexpr PassDesc p0 = fft_pass_desc(M, 0), p1 = fft_pass_desc(M, 1), p2 = fft_pass_desc(M, 2);
+  constexpr int NP = fft_npasses(M);
+  fft_pass<M, TPF, p0.R, p0.NS, true, false, INV, 0>(x, sm, tw, t, bar);
+  fft_pass<M, TPF, p1.R, p1.NS, false, false, INV, tw_offset(M, 1)>(x, sm, tw, t, bar);
+  fft_pass<M, TPF, p2.R, p2.NS, false, NP == 3, INV, tw_offset(M, 2)>(x, sm, tw, t, bar);
+  if constexpr (NP == 4) {
+    constexpr PassDesc p3 = fft_pass_desc(M, 3);
+    fft_pass<M, TPF, p3.R, p3.NS, false, true, INV, tw_offset(M, 3)>(x, sm, tw, t, bar);
   }
 }
 

@@ -58,13 +58,16 @@ srk_status noalloc_scratch(void** out) {
   return SRK_OK;
 }
 
-// exp(-2 pi i m / M) in double, rounded once to float.
+// The FFT twiddle table (per-pass blocks, tw_entry), exp(-2 pi i num/den)
+// in double, rounded once to float.
 __global__ void k_noalloc_twiddles(float2* __restrict__ tw, int M) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= M) return;
+  int num = 0, den = 1;
+  tw_entry(M, m, num, den);
   double s, c;
-  sincospi(2.0 * (double)m / (double)M, &s, &c);
-  tw[m] = make_float2((float)c, (float)-s);
+  sincospi(2.0 * (double)num / (double)den, &s, &c);
+  tw[m] = m < tw_entries(M) ? make_float2((float)c, (float)-s) : make_float2(0.f, 0.f);
 }
 
 // Reference half spectrum (size M) -> engine layout, Hermitian extension,

@@ -391,9 +391,14 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   *p->mailbox_spins = 0;
   if ((err = cudaEventCreateWithFlags(&p->mailbox_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup(cuda_status(err, "event creation"));
-  std::vector<float2> tw(M);
-  const std::vector<double2> t64 = twiddles64(M);
-  for (int m = 0; m < M; ++m) tw[m] = make_float2((float)t64[m].x, (float)-t64[m].y);  // exp(-2 pi i m/M)
+  // per-pass twiddle blocks (tw_entry), exp(-2 pi i num/den) in double, rounded once
+  std::vector<float2> tw(M, make_float2(0.f, 0.f));
+  for (int m = 0; m < tw_entries(M); ++m) {
+    int num = 0, den = 1;
+    tw_entry(M, m, num, den);
+    const double ang = 2.0 * 3.14159265358979323846 * (double)num / (double)den;
+    tw[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  }
   if ((err = cudaMemcpy(p->tw, tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice)) != cudaSuccess)
     return cleanup(cuda_status(err, "twiddle upload"));
   *out = p;
