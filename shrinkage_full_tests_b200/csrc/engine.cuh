@@ -119,6 +119,10 @@ __device__ __forceinline__ float grad_y(const T* f, int N, int gx, int gy) {
   return (d - u) * 0.5f;
 }
 
+// a*b + c*d with one fixed rounding sequence, so every kernel that inlines
+// an epilogue produces bit-identical results.
+__device__ __forceinline__ float dot2(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
+
 struct TileRef {
   int b, x0, y0;  // image index and tile origin in virtual input coordinates
   bool live;
@@ -161,7 +165,7 @@ __device__ __forceinline__ float h_at(const OpArgs& a, int b, int k, int px, int
   const T* df = static_cast<const T*>(a.dI) + (long long)b * a.N * a.N;
   const float dv = ldf(static_cast<const T*>(a.dv), vo);
   const float dg = (k == 0) ? grad_x(df, a.N, qx, qy) : grad_y(df, a.N, qx, qy);
-  return dv * g + v * dg;
+  return dot2(dv, g, v, dg);
 }
 
 // Column x of one real tile of image `img` (forward-type ops): values at
@@ -311,7 +315,7 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
             float fx = 0.f, fy = 0.f;
             if (vm >> i & 1u) gc.at(i, fx, fy);
             float& o = h ? z0[i].y : z0[i].x;
-            o = o * fx + (h ? z1[i].y : z1[i].x) * fy;
+            o = dot2(o, fx, h ? z1[i].y : z1[i].x, fy);
           }
 #pragma unroll
           for (int i = 0; i < EPT; ++i)
@@ -350,7 +354,7 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
           gf.at(i, fx, fy);
           gd.at(i, dfx, dfy);
         }
-        z0[i].x = z0[i].y * fx + z1[i].y * fy + z0[i].x * dfx + z1[i].x * dfy;
+        z0[i].x = __fmaf_rn(z1[i].x, dfy, __fmaf_rn(z0[i].x, dfx, dot2(z0[i].y, fx, z1[i].y, fy)));
       }
 #pragma unroll
       for (int i = 0; i < EPT; ++i)
@@ -393,56 +397,86 @@ __host__ __device__ constexpr int lpu_of() { return kThreads / tpf_of<M>(); }
 
 // ---- staged gradients -------------------------------------------------------------
 // The LPU output columns of a P3 unit need the image columns gx-1 ..
-// gx+LPU and rows gy-1 .. gy+S.  They are staged cooperatively (coalesced,
-// every load in flight) into shared memory: window column c <-> image
-// column x0 + e - 1 + c, window row r <-> image row y0 + e - 1 + r;
-// out-of-image elements are zero (the central-difference rule).
-__host__ __device__ inline int gwin_pitch(int S) { return (S + 2 + 1) & ~1; }
-// (LPU + 2) * gwin_pitch(S) floats <= (LPU + 2) * (M + 3) <= 2 * LPU * (M + M/16 + 2):
-// one image's window always fits the LPU staging rows of the second field.
+// gx+LPU and rows gy-1 .. gy+S.  They are staged into shared memory, one
+// warp per window column: window column c <-> image column x0 + e - 1 + c;
+// window row r <-> image row gy0 + r, gy0 = y0 + e - 1, stored at column
+// offset off + r.  Out-of-image elements are zero (the central-difference
+// rule).  With 16-byte copies the column starts at the aligned row
+// gy0 - off (off = gy0 mod 4); otherwise off = 0.  The pitch is a multiple
+// of 4 floats (16-byte aligned columns).
+__host__ __device__ inline int gwin_pitch(int S) { return (S + 8) & ~3; }
+// (LPU + 2) * gwin_pitch(S) floats <= (LPU + 2) * (M + 4) <= 2 * LPU * (M + M/16 + 2)
+// for S <= M - 2: one image's window always fits the LPU staging rows of the
+// second field.
+struct GradWin {
+  int gx0, gy0;  // image coordinates of window column 0, row 0
+  int ncol, S;   // columns, and S + 2 rows
+  int HP, off;   // column pitch (floats), offset of row 0 in a column
+};
 
+// Synchronous staging (any storage type; values converted to float).
 template <typename T>
-__device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int N, int gx0, int gy0, int S,
-                                                  int ncol, float* __restrict__ dst) {
-  const int HP = gwin_pitch(S);
-  const int H = S + 2;
-  // (c, r) of element threadIdx.x + j*kThreads, advanced without division
-  const int dc = kThreads / H, dr = kThreads - dc * H;
-  int c = threadIdx.x / H, r = threadIdx.x - c * H;
-  for (; c < ncol; c += dc, r += dr) {
-    if (r >= H) { r -= H; ++c; if (c >= ncol) break; }
-    const int gx = gx0 + c, gy = gy0 + r;
-    dst[c * HP + r] = (gx >= 0 && gx < N && gy >= 0 && gy < N) ? ldf(img, (long long)gx * N + gy) : 0.f;
+__device__ __forceinline__ void stage_grad_window(const T* __restrict__ img, int N, const GradWin& gw,
+                                                  float* __restrict__ dst) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int H = gw.S + 2;
+  for (int c = warp; c < gw.ncol; c += kWarps) {
+    const int gx = gw.gx0 + c;
+    const bool colin = gx >= 0 && gx < N;
+    const T* col = img + (long long)(colin ? gx : 0) * N;
+    float* d = dst + c * gw.HP;
+    for (int r = lane; r < H; r += 32) {
+      const int gy = gw.gy0 + r;
+      d[r] = (colin && gy >= 0 && gy < N) ? ldf(col, gy) : 0.f;
+    }
   }
 }
 
-// The same window copied with asynchronous 4-byte global->shared copies
-// (cp.async, zero fill outside the image): the caller commits the group and
-// waits for it later, so the loads overlap other work.  FP32 images only.
+// Asynchronous staging with cp.async (FP32 images): the caller commits the
+// group and waits for it later, so the loads overlap other work.
 __device__ __forceinline__ void cp_async4_zfill(float* dst, const float* src, bool valid) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16_zfill(float* dst, const float* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ void stage_grad_window_async(const float* __restrict__ img, int N, int gx0, int gy0, int S,
-                                                        int ncol, float* __restrict__ dst) {
-  const int HP = gwin_pitch(S);
-  const int H = S + 2;
-  const int dc = kThreads / H, dr = kThreads - dc * H;
-  int c = threadIdx.x / H, r = threadIdx.x - c * H;
-  for (; c < ncol; c += dc, r += dr) {
-    if (r >= H) { r -= H; ++c; if (c >= ncol) break; }
-    const int gx = gx0 + c, gy = gy0 + r;
-    const bool in = gx >= 0 && gx < N && gy >= 0 && gy < N;
-    cp_async4_zfill(dst + c * HP + r, in ? img + (long long)gx * N + gy : img, in);
+// vec16: 16-byte chunks (needs N % 4 == 0 and a 16-byte aligned image, so
+// every chunk lies wholly inside or wholly outside the image); else 4-byte
+// copies.
+__device__ __forceinline__ void stage_grad_window_async(const float* __restrict__ img, int N, const GradWin& gw,
+                                                        bool vec16, float* __restrict__ dst) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < gw.ncol; c += kWarps) {
+    const int gx = gw.gx0 + c;
+    const bool colin = gx >= 0 && gx < N;
+    const float* col = img + (long long)(colin ? gx : 0) * N;
+    float* d = dst + c * gw.HP;
+    if (vec16) {
+      const int gya = gw.gy0 - gw.off;
+      const int nch = (gw.off + gw.S + 2 + 3) >> 2;
+      for (int q = lane; q < nch; q += 32) {
+        const int gy = gya + 4 * q;
+        const bool in = colin && gy >= 0 && gy < N;
+        cp_async16_zfill(d + 4 * q, in ? col + gy : img, in);
+      }
+    } else {
+      for (int r = lane; r < gw.S + 2; r += 32) {
+        const int gy = gw.gy0 + r;
+        const bool in = colin && gy >= 0 && gy < N;
+        cp_async4_zfill(d + r, in ? col + gy : img, in);
+      }
+    }
   }
 }
 // Floats of one staged window at tile size M (S <= M - 2 when erosion >= 1).
 template <int M>
-__host__ __device__ constexpr int p3_window_floats() { return (lpu_of<M>() + 2) * M; }
+__host__ __device__ constexpr int p3_window_floats() { return (lpu_of<M>() + 2) * (M + 4); }
 // P3 of the three-launch schedule prefetches the first window asynchronously
 // into a buffer of its own (forward / tangent epilogues on FP32 images).
 template <int OP, typename T>
@@ -457,18 +491,18 @@ __host__ __device__ constexpr bool p3_async_window() {
 // terms.  z0 stays stashed in the line's padded row (z0s = row + t +
 // (t >> 4), element i at z0s[(TPF + TPF/16) i]) to keep registers free.
 template <int M, int OP, typename T>
-__device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, int w, int x, int line, int t, int h,
-                                                float2* __restrict__ z0s, const float2 (&z1)[M / tpf_of<M>()],
-                                                const float* __restrict__ win, int HP) {
+__device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, const TileRef& tr, int x, int line,
+                                                int t, int h, float2* __restrict__ z0s,
+                                                const float2 (&z1)[M / tpf_of<M>()], const float* __restrict__ win,
+                                                const GradWin& gw) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int RSP = TPF + TPF / 16;
   const int W = a.W;
-  const int rb = t - g.e + 1;  // window row of element 0: y - e + 1, y = t
-  const float* cm = win + line * HP + rb;  // image column gx - 1
-  const float* cc = cm + HP;               // gx
-  const float* cp = cc + HP;               // gx + 1
-  const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
+  const int rb = gw.off + t - g.e + 1;        // window row of element 0: y - e + 1, y = t
+  const float* cm = win + line * gw.HP + rb;  // image column gx - 1
+  const float* cc = cm + gw.HP;               // gx
+  const float* cp = cc + gw.HP;               // gx + 1
   const int ox = tr.x0 + x - g.e;
   if (!tr.live || ox >= g.Wout) return;
   const unsigned vm = valid_rows<M>(g, tr.y0, t);
@@ -477,6 +511,20 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
     T* __restrict__ R = static_cast<T*>(a.out0);
     T* __restrict__ UX = static_cast<T*>(a.out_ux);
     T* __restrict__ UY = static_cast<T*>(a.out_uy);
+    if (R && !UX && !UY && vm == (1u << EPT) - 1u) {
+      // every row valid, R only: the common case
+      T* __restrict__ Rp = R + ob;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const float2 z0i = z0s[RSP * i];
+        const float ux = h ? z0i.y : z0i.x;
+        const float uy = h ? z1[i].y : z1[i].x;
+        const float fx = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
+        const float fy = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+        stf(Rp, TPF * i, dot2(ux, fx, uy, fy));
+      }
+      return;
+    }
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       if (!(vm >> i & 1u)) continue;
@@ -488,7 +536,7 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
       if (R) {
         const float fx = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
         const float fy = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
-        stf(R, ob + TPF * i, ux * fx + uy * fy);
+        stf(R, ob + TPF * i, dot2(ux, fx, uy, fy));
       }
     }
   } else {
@@ -501,10 +549,10 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
       const float dy_ = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
       float2 z0i = z0s[RSP * i];
       if (h == 0) {
-        z0i.y = z0i.y * dx_ + z1[i].y * dy_;
+        z0i.y = dot2(z0i.y, dx_, z1[i].y, dy_);
         z0s[RSP * i] = z0i;
       } else {
-        stf(static_cast<T*>(a.out0), ob + TPF * i, z0i.y + z0i.x * dx_ + z1[i].x * dy_);
+        stf(static_cast<T*>(a.out0), ob + TPF * i, __fmaf_rn(z1[i].x, dy_, __fmaf_rn(z0i.x, dx_, z0i.y)));
       }
     }
   }
@@ -675,14 +723,29 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   const int P = s2_pitch(g.S);
   const int x0 = xb * LPU;
   const int bar = 1 + line;
-  // window h: image (pair member h, or f / df) columns x0+e-1 .. x0+e+LPU, rows y0+e-1 .. y0+e+S
+  // window of round h: image (pair member h, or f / df) columns
+  // x0+e-1 .. x0+e+LPU, rows y0+e-1 .. y0+e+S
+  auto window_of = [&](int h, const TileRef& tr, bool vec16) {
+    GradWin gw;
+    gw.gx0 = tr.x0 + x0 + a.e - 1;
+    gw.gy0 = tr.y0 + a.e - 1;
+    gw.ncol = LPU + 2;
+    gw.S = g.S;
+    gw.HP = gwin_pitch(g.S);
+    gw.off = vec16 ? (gw.gy0 & 3) : 0;
+    return gw;
+  };
+  auto tile_h = [&](int h) { return tile_of(g, OP == OP_FWD ? 2 * w + h : w); };
+  auto image_h = [&](int h) { return static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI); };
+  // 16-byte window copies: N % 4 == 0 and 16-byte aligned images
+  const bool vec16 = ASYNC && (a.N & 3) == 0 && (reinterpret_cast<uintptr_t>(a.I) & 15) == 0 &&
+                     (OP != OP_JVP || (reinterpret_cast<uintptr_t>(a.dI) & 15) == 0);
   auto issue_window = [&](int h, float* dst) {
     if constexpr (ASYNC) {
-      const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
-      const float* img = static_cast<const float*>(OP == OP_FWD || h == 0 ? a.I : a.dI);
+      const TileRef tr = tile_h(h);
       if (tr.live)
-        stage_grad_window_async(img + (long long)tr.b * a.N * a.N, a.N, tr.x0 + x0 + a.e - 1, tr.y0 + a.e - 1, g.S,
-                                LPU + 2, dst);
+        stage_grad_window_async(reinterpret_cast<const float*>(image_h(h)) + (long long)tr.b * a.N * a.N, a.N,
+                                window_of(h, tr, vec16), vec16, dst);
       cp_async_commit();
     }
   };
@@ -716,16 +779,17 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
       // window 0 has been arriving in its own buffer; window 1 goes to the
       // second field's rows once every line is done with them
       float* win1 = reinterpret_cast<float*>(rows + LPU * RS);
-      const int HP = gwin_pitch(g.S);
       float2* z0s = row0 + t + (t >> 4);
       __syncthreads();
       issue_window(1, win1);
       cp_async_wait<1>();
       __syncthreads();
-      if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, 0, z0s, z1, win0, HP);
+      const TileRef tr0 = tile_h(0);
+      if (active) epilogue_staged<M, OP, T>(a, g, tr0, xv + g.e, line, t, 0, z0s, z1, win0, window_of(0, tr0, vec16));
       cp_async_wait<0>();
       __syncthreads();
-      if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, 1, z0s, z1, win1, HP);
+      const TileRef tr1 = tile_h(1);
+      if (active) epilogue_staged<M, OP, T>(a, g, tr1, xv + g.e, line, t, 1, z0s, z1, win1, window_of(1, tr1, vec16));
       return;
     }
   }
@@ -733,18 +797,15 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
     if (a.e >= 1) {
       // two rounds, one image window each, in the second field's rows
       float* win = reinterpret_cast<float*>(rows + LPU * RS);
-      const int HP = gwin_pitch(g.S);
       float2* z0s = row0 + t + (t >> 4);
 #pragma unroll 1
       for (int h = 0; h < 2; ++h) {
         __syncthreads();  // rows of field 1 no longer used (round 0) / window consumed (round 1)
-        const TileRef tr = tile_of(g, OP == OP_FWD ? 2 * w + h : w);
-        const T* img = static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI);
-        if (tr.live)
-          stage_grad_window<T>(img + (long long)tr.b * a.N * a.N, a.N, tr.x0 + x0 + a.e - 1, tr.y0 + a.e - 1, g.S,
-                               LPU + 2, win);
+        const TileRef tr = tile_h(h);
+        const GradWin gw = window_of(h, tr, false);
+        if (tr.live) stage_grad_window<T>(image_h(h) + (long long)tr.b * a.N * a.N, a.N, gw, win);
         __syncthreads();
-        if (active) epilogue_staged<M, OP, T>(a, g, w, xv + g.e, line, t, h, z0s, z1, win, HP);
+        if (active) epilogue_staged<M, OP, T>(a, g, tr, xv + g.e, line, t, h, z0s, z1, win, gw);
       }
       return;
     }

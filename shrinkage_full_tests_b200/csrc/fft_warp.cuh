@@ -26,14 +26,17 @@
 
 namespace srk {
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex arithmetic with every rounding spelled out (no compiler
+// contraction of a product into a later sum): each kernel that inlines a
+// transform computes bit-identical results, whatever the schedule.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y)); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_float2(__fmaf_rn(a.x, b.x, -__fmul_rn(a.y, b.y)), __fmaf_rn(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
 // a * conj(b)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
-  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+  return make_float2(__fmaf_rn(a.x, b.x, __fmul_rn(a.y, b.y)), __fmaf_rn(a.y, b.x, -__fmul_rn(a.x, b.y)));
 }
 template <bool INV>
 __device__ __forceinline__ float2 twmul(float2 a, float2 w) {
@@ -54,17 +57,17 @@ __device__ __forceinline__ float2 rot16(float2 v) {
   } else if constexpr (m == 4) {                  // -i (forward) / +i (inverse)
     return INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
   } else if constexpr (m == 2) {                  // (1 -+ i)/sqrt2
-    return INV ? make_float2((v.x - v.y) * R2, (v.x + v.y) * R2)
-               : make_float2((v.x + v.y) * R2, (v.y - v.x) * R2);
+    const float p = __fadd_rn(v.x, v.y), q = __fsub_rn(v.x, v.y);
+    return INV ? make_float2(__fmul_rn(q, R2), __fmul_rn(p, R2)) : make_float2(__fmul_rn(p, R2), __fmul_rn(-q, R2));
   } else if constexpr (m == 6) {                  // (-1 -+ i)/sqrt2
-    return INV ? make_float2(-(v.x + v.y) * R2, (v.x - v.y) * R2)
-               : make_float2((v.y - v.x) * R2, -(v.x + v.y) * R2);
+    const float p = __fadd_rn(v.x, v.y), q = __fsub_rn(v.x, v.y);
+    return INV ? make_float2(__fmul_rn(-p, R2), __fmul_rn(q, R2)) : make_float2(__fmul_rn(-q, R2), __fmul_rn(-p, R2));
   } else {
     constexpr float c = (m == 1) ? C1 : (m == 3) ? S1 : (m == 5) ? -S1 : -C1;
     constexpr float s = (m == 1) ? S1 : (m == 3) ? C1 : (m == 5) ? C1 : S1;
     // forward: v*(c - i s); inverse: v*(c + i s)
-    return INV ? make_float2(v.x * c - v.y * s, v.y * c + v.x * s)
-               : make_float2(v.x * c + v.y * s, v.y * c - v.x * s);
+    return INV ? make_float2(__fmaf_rn(v.x, c, -__fmul_rn(v.y, s)), __fmaf_rn(v.y, c, __fmul_rn(v.x, s)))
+               : make_float2(__fmaf_rn(v.x, c, __fmul_rn(v.y, s)), __fmaf_rn(v.y, c, -__fmul_rn(v.x, s)));
   }
 }
 
