@@ -563,10 +563,16 @@ __device__ __forceinline__ void load_twiddles(float2* tw, const float2* __restri
   for (int i = threadIdx.x; i < tw_entries(M); i += blockDim.x) tw[i] = twg[i];
 }
 
-// Staging rows: stride RW + 2 float2 so the rows of a transposing copy fall
-// into different banks.
+// Staging rows: fft_row_words(M) or a little more, so that the rows of a
+// transposing copy fall into different banks.
 template <int M>
-__host__ __device__ constexpr int row_stride() { return fft_row_words(M) + 2; }
+__host__ __device__ constexpr int row_stride() {
+  // stage_rows writes 2 (LPU = 4) or 4 (LPU = 8) rows per half-warp: their
+  // strides must land on disjoint banks (RS = 4 or 2 mod 8 complex values)
+  int w = fft_row_words(M) + 1;
+  while (w % 8 != (lpu_of<M>() == 4 ? 4 : 2)) ++w;
+  return w;
+}
 // S2 rows are padded to a multiple of 8 columns (16-byte aligned float4 reads).
 __host__ __device__ inline int s2_pitch(int S) { return (S + 7) & ~7; }
 

@@ -43,8 +43,24 @@ __device__ __forceinline__ float2 twmul(float2 a, float2 w) {
   return INV ? cmulc(a, w) : cmul(a, w);
 }
 
+// Padded positions in a transform's shared row.  fft_pad is the layout of
+// rows handed between phases (staging, stashes) and of the first exchange;
+// the later exchanges of a transform use their own padding (exch_pad),
+// chosen so that the 8-byte writes of that exchange and the reads after it
+// keep every half-warp on distinct banks.
 __host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int fft_row_words(int M) { return M + M / 16; }
+template <int K>
+__host__ __device__ constexpr int padk(int i) {
+  return K == 0 ? i + (i >> 4) : K == 1 ? i + 8 * (i >> 6) : i + 4 * (i >> 4);
+}
+// Padding of the exchange that follows pass p of an M-point transform.
+__host__ __device__ constexpr int exch_pad(int M, int p) { return p == 1 ? (M == 128 ? 2 : 1) : 0; }
+// Row length (complex values) that holds every padding used on the row.
+__host__ __device__ constexpr int fft_row_words(int M) {
+  const int a = fft_pad(M - 1) + 1;
+  const int b = (M == 128 ? padk<2>(M - 1) : padk<1>(M - 1)) + 1;
+  return a > b ? a : b;
+}
 
 // Multiply by W_16^m = exp(-+ i*pi*m/8) for a compile-time m in [0,8).
 template <int m, bool INV>
@@ -165,16 +181,24 @@ template <int R, int NS, int TPF>
 __host__ __device__ constexpr int pass_C(int b, int r) {
   return NS >= TPF ? ((TPF * b) / NS) * NS * R + (TPF * b) % NS + r * NS : TPF * b * R + r * NS;
 }
-// fft_pad(P + C) == fft_pad(P) + fft_pad(C) for every thread, butterfly and
+// padk<K>(P + C) == padk<K>(P) + padk<K>(C) for every thread, butterfly and
 // leg: then every shared-memory write is (per-thread base) + (immediate).
-template <int M, int R, int NS, int TPF>
+template <int M, int R, int NS, int TPF, int K>
 __host__ __device__ constexpr bool pad_separable() {
   for (int t = 0; t < TPF; ++t)
     for (int b = 0; b < M / TPF / R; ++b)
       for (int r = 0; r < R; ++r) {
         const int P = pass_P<R, NS, TPF>(t), C = pass_C<R, NS, TPF>(b, r);
-        if (fft_pad(P + C) != fft_pad(P) + fft_pad(C)) return false;
+        if (padk<K>(P + C) != padk<K>(P) + padk<K>(C)) return false;
       }
+  return true;
+}
+// The same for the reads X[t + TPF i].
+template <int M, int TPF, int K>
+__host__ __device__ constexpr bool read_separable() {
+  for (int t = 0; t < TPF; ++t)
+    for (int i = 0; i < M / TPF; ++i)
+      if (padk<K>(t + TPF * i) != padk<K>(t) + padk<K>(TPF * i)) return false;
   return true;
 }
 
@@ -190,22 +214,24 @@ __device__ __forceinline__ void group_sync(int bar) {
 }
 
 // One Stockham pass.  sm: this transform's padded exchange row; tw: W_M table.
-template <int M, int TPF, int R, int NS, bool FIRST, bool LAST, bool INV, int TWOFF>
+// PIN / POUT: padding (padk) of the exchange read before / written after
+// the pass.
+template <int M, int TPF, int R, int NS, bool FIRST, bool LAST, bool INV, int TWOFF, int PIN, int POUT>
 __device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restrict__ sm,
                                          const float2* __restrict__ tw, int t, int bar) {
   constexpr int EPT = M / TPF;
   constexpr int NB = EPT / R;
   static_assert(EPT % R == 0, "radix must divide elements per thread");
-  static_assert(LAST || pad_separable<M, R, NS, TPF>(), "padded write index must split into base + immediate");
+  static_assert(LAST || pad_separable<M, R, NS, TPF, POUT>(), "padded write index must split into base + immediate");
+  static_assert(FIRST || read_separable<M, TPF, PIN>(), "padded read index must split into base + immediate");
   if constexpr (!FIRST) {
-    // fft_pad(t + TPF i) = t + (t >> 4) + (TPF + TPF/16) i
-    const float2* rd = sm + t + (t >> 4);
+    const float2* rd = sm + padk<PIN>(t);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) x[i] = rd[(TPF + TPF / 16) * i];
+    for (int i = 0; i < EPT; ++i) x[i] = rd[padk<PIN>(TPF * i)];
     group_sync<TPF>(bar);
   }
   float2* wr = nullptr;
-  if constexpr (!LAST) wr = sm + fft_pad(pass_P<R, NS, TPF>(t));
+  if constexpr (!LAST) wr = sm + padk<POUT>(pass_P<R, NS, TPF>(t));
   const float2* twp = tw + TWOFF;  // this pass's W_{NS R}^k block
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
@@ -226,7 +252,7 @@ __device__ __forceinline__ void fft_pass(float2 (&x)[M / TPF], float2* __restric
       for (int r = 0; r < R; ++r) x[b + r * NB] = a[r];
     } else {
 #pragma unroll
-      for (int r = 0; r < R; ++r) wr[fft_pad(pass_C<R, NS, TPF>(b, r))] = a[r];
+      for (int r = 0; r < R; ++r) wr[padk<POUT>(pass_C<R, NS, TPF>(b, r))] = a[r];
     }
   }
   if constexpr (!LAST) group_sync<TPF>(bar);
@@ -247,12 +273,13 @@ __device__ __forceinline__ void fft(float2 (&x)[M / TPF], float2* __restrict__ s
   static_assert(M == 128 || M == 256 || M == 512, "unsupported FFT length");
   constexpr PassDesc p0 = fft_pass_desc(M, 0), p1 = fft_pass_desc(M, 1), p2 = fft_pass_desc(M, 2);
   constexpr int NP = fft_npasses(M);
-  fft_pass<M, TPF, p0.R, p0.NS, true, false, INV, 0>(x, sm, tw, t, bar);
-  fft_pass<M, TPF, p1.R, p1.NS, false, false, INV, tw_offset(M, 1)>(x, sm, tw, t, bar);
-  fft_pass<M, TPF, p2.R, p2.NS, false, NP == 3, INV, tw_offset(M, 2)>(x, sm, tw, t, bar);
+  constexpr int X0 = exch_pad(M, 0), X1 = exch_pad(M, 1), X2 = exch_pad(M, 2);
+  fft_pass<M, TPF, p0.R, p0.NS, true, false, INV, 0, X0, X0>(x, sm, tw, t, bar);
+  fft_pass<M, TPF, p1.R, p1.NS, false, false, INV, tw_offset(M, 1), X0, X1>(x, sm, tw, t, bar);
+  fft_pass<M, TPF, p2.R, p2.NS, false, NP == 3, INV, tw_offset(M, 2), X1, X2>(x, sm, tw, t, bar);
   if constexpr (NP == 4) {
     constexpr PassDesc p3 = fft_pass_desc(M, 3);
-    fft_pass<M, TPF, p3.R, p3.NS, false, true, INV, tw_offset(M, 3)>(x, sm, tw, t, bar);
+    fft_pass<M, TPF, p3.R, p3.NS, false, true, INV, tw_offset(M, 3), X2, X2>(x, sm, tw, t, bar);
   }
 }
 
