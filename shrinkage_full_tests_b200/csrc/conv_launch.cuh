@@ -54,8 +54,12 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
     SRK_CUDA(cudaMemcpyAsync(p->mailbox, &p->ctl->abort, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     SRK_CUDA(cudaMemcpyAsync(p->mailbox_spins, &p->ctl->spins, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s));
-    SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
-    p->mailbox_pending = true;
+    if (stream_capturing(s)) {
+      p->graph_mailbox = true;  // checked by srk_plan_sync after a replay
+    } else {
+      SRK_CUDA(cudaEventRecord(p->mailbox_ev, s));
+      p->mailbox_pending = true;
+    }
     p->last_grid = grid;
     p->last_launches = 1;
     p->last_lag = pp.lag;

@@ -18,6 +18,12 @@
 #include "engine.cuh"
 
 namespace srk {
+// True while `s` is being captured into a CUDA graph: no event queries or
+// host synchronisation may happen then.
+inline bool stream_capturing(cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone;
+}
 
 inline thread_local std::string g_last_error;
 
@@ -66,6 +72,7 @@ struct srk_plan_s {
   unsigned int* mailbox = nullptr;     // pinned host copy of (abort, where)
   cudaEvent_t mailbox_ev = nullptr;
   bool mailbox_pending = false;
+  bool graph_mailbox = false;          // a captured persistent launch writes the mailbox on replay
   unsigned long long spin_limit = 1ull << 25;
   unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
   int persist_lag = 0, persist_grid = 0, persist_prefetch = 0;

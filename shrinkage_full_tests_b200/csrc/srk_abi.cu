@@ -236,8 +236,9 @@ srk_status check_mailbox(srk_plan_s* p) {
   return SRK_OK;
 }
 
-srk_status enter(srk_plan_s* p) {
+srk_status enter(srk_plan_s* p, cudaStream_t s) {
   SRK_TRY(set_device(p));
+  if (stream_capturing(s)) return SRK_OK;
   return check_mailbox(p);
 }
 
@@ -455,13 +456,21 @@ srk_status srk_plan_sync(srk_plan p, srk_stream_t s) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(set_device(p));
   SRK_CUDA(cudaStreamSynchronize(s));
+  if (p->graph_mailbox && p->mailbox[0]) {
+    // written by a persistent launch replayed from a captured graph
+    const unsigned int where = p->mailbox[1];
+    p->mailbox[0] = 0;
+    p->mailbox_pending = false;
+    return fail(SRK_ERR_TIMEOUT, "a bounded device-side wait gave up (site %u); that call's outputs are incomplete",
+                where);
+  }
   return check_mailbox(p);
 }
 
 srk_status srk_debug_wait_selftest(srk_plan p, unsigned long long spin_limit, srk_stream_t s) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   if (spin_limit == 0 || spin_limit > (1ull << 26)) return fail(SRK_ERR_INVALID_ARG, "spin_limit out of range");
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_CUDA(cudaMemsetAsync(p->ctl, 0, sizeof(Ctl), s));
   k_wait_selftest<<<1, 32, 0, s>>>(p->ctl, spin_limit);
   SRK_CUDA(cudaGetLastError());
@@ -540,7 +549,7 @@ srk_status op_training_forward(const void* E, const void* I, const void* gx, con
   SRK_NONNULL(R);
   if (p->spectra_M != N && (gx || gy))
     return fail(SRK_ERR_INVALID_ARG, "training spectra must be at size N=%d (plan has spectra_M=%d)", N, p->spectra_M);
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R;
@@ -553,7 +562,7 @@ srk_status op_forward_oas(const void* E, const void* I, const void* gx, const vo
   SRK_NONNULL(E);
   SRK_NONNULL(I);
   SRK_NONNULL(R);
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R; a.out_ux = ux; a.out_uy = uy;
@@ -569,7 +578,7 @@ srk_status op_adjoint(const void* v, const void* ux, const void* uy, const void*
   SRK_NONNULL(I);
   SRK_NONNULL(dLdI);
   SRK_NONNULL(dLdE);
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   SRK_TRY(adj_wrt_f(p, nullptr, nullptr, v, ux, uy, 1, dLdI, s));
   return run_adj_g(p, v, nullptr, I, nullptr, 1, p->conv == SRK_ADJ_TRUE, dLdE, s);
@@ -583,7 +592,7 @@ srk_status op_tangent(const void* f, const void* g, const void* df, const void* 
   SRK_NONNULL(df);
   SRK_NONNULL(dg);
   SRK_NONNULL(dh);
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
@@ -602,7 +611,7 @@ srk_status op_tangent_adjoint(const void* f, const void* g, const void* df, cons
   SRK_NONNULL(dlam);
   SRK_NONNULL(dLam_f);
   SRK_NONNULL(dLam_g);
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
   const size_t ww = (size_t)p->W * p->W;
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
@@ -620,7 +629,7 @@ srk_status op_forward(const void* f, const void* g, int B, srk_stream_t s, void*
   SRK_NONNULL(g);
   SRK_NONNULL(h);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   OpArgs a = base_args(p);
   a.E = g; a.I = f; a.out0 = h;
   return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, B), false, s);
@@ -636,7 +645,7 @@ srk_status op_vjp(const void* v, const void* f, const void* g, int B, srk_stream
   SRK_NONNULL(dLdf);
   SRK_NONNULL(dLdg);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   const size_t ww = (size_t)p->W * p->W * B;
   SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
   OpArgs a = base_args(p);
@@ -657,7 +666,7 @@ srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, 
   SRK_NONNULL(dg);
   SRK_NONNULL(dh);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
-  SRK_TRY(enter(p));
+  SRK_TRY(enter(p, s));
   OpArgs a = base_args(p);
   a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
   return launch_conv_dt<OP_JVP>(p, a, fwd_geom(p, B), false, s);
