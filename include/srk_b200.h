@@ -188,6 +188,29 @@ srk_status srk_vjp(const float* d_v, const float* d_f, const float* d_g, int B, 
 srk_status srk_jvp(const float* d_f, const float* d_g, const float* d_df, const float* d_dg, int B,
                    srk_stream_t stream, float* d_dh, srk_plan plan);
 
+/* ---- ragged batches: B images of different sizes in one launch -----------
+ * The reference runs one image per call (srkForwardOaS, adjointSRK,
+ * shrinkageTangentOaS, shrinkageTangentAdjointOaS above); these forms take
+ * B images whose sizes are given by Ns, a HOST array of B sizes with
+ * 2*erosion+1 <= Ns[b] <= the plan's N, all with the plan's erosion, dx,
+ * tile size and spectra.  Every buffer holds the images one after another,
+ * column-major: N-sized buffers Ns[b]^2 elements per image, W-sized ones
+ * (Ns[b] - 2*erosion)^2.  The tile tables are uploaded once per distinct Ns
+ * (stream ordered); issue the ragged calls of one plan on one stream. */
+srk_status srk_forward_oas_ragged(const float* d_E, const float* d_I, const void* d_Gx_freq,
+                                  const void* d_Gy_freq, int B, const int* Ns, int erosion, float dx,
+                                  srk_stream_t stream, float* d_R, srk_plan plan);
+srk_status srk_adjoint_ragged(const float* d_v, const float* d_ux, const float* d_uy, const float* d_I,
+                              const void* d_Gx_freq, const void* d_Gy_freq, int B, const int* Ns, int erosion,
+                              float dx, srk_stream_t stream, float* d_dLdI, float* d_dLdE, srk_plan plan);
+srk_status srk_tangent_ragged(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                              const void* d_Gx_freq, const void* d_Gy_freq, int B, const int* Ns, int erosion,
+                              float dx, srk_stream_t stream, float* d_dh, srk_plan plan);
+srk_status srk_tangent_adjoint_ragged(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                                      const float* d_lam_h, const float* d_dlam_h, const void* d_Gx_freq,
+                                      const void* d_Gy_freq, int B, const int* Ns, int erosion, float dx,
+                                      srk_stream_t stream, float* d_dLam_f, float* d_dLam_g, srk_plan plan);
+
 /* ---- critical dimension (CD) of line/space signals ------------------------
  * MeasureCD_Batched (third_party/src/metricUtil/cd_measure_util.cu:310-437)
  * in one kernel per signal: L-fold windowed-sinc upsampling (half width A),

@@ -86,6 +86,10 @@ _SIGS = {
     "srk_forward": [_P, _P, _I, _P, _P, _P],
     "srk_vjp": [_P, _P, _P, _I, _P, _P, _P, _P],
     "srk_jvp": [_P, _P, _P, _P, _I, _P, _P, _P],
+    "srk_forward_oas_ragged": [_P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P],
+    "srk_adjoint_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P, _P],
+    "srk_tangent_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P],
+    "srk_tangent_adjoint_ragged": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P, _P],
 }
 # storage-typed forms (void* buffers in the plan's dtype): same argument types
 for _n in ("srk_training_forward", "srk_forward_oas", "srk_adjoint", "srk_tangent", "srk_tangent_adjoint",
@@ -233,6 +237,39 @@ def shrinkageTangentAdjointOaS(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_freq, N,
     _check(_entry("srk_tangent_adjoint", ws)(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
                                              _ptr(Gx_freq), _ptr(Gy_freq), N, W, erosion, dx, _stream(stream),
                                              _ptr(dLam_f), _ptr(dLam_g), ws.handle))
+
+
+def _sizes(Ns):
+    Ns = [int(n) for n in Ns]
+    return len(Ns), (ctypes.c_int * max(1, len(Ns)))(*Ns)
+
+
+# ---- ragged batches: images of different N concatenated in every buffer
+# (Ns[b]^2 elements per image in N-sized buffers, (Ns[b]-2e)^2 in W-sized ones)
+def srkForwardOaSRagged(E, I, Gx_freq, Gy_freq, Ns, erosion, dx, stream, R, ws):
+    B, arr = _sizes(Ns)
+    _check(lib().srk_forward_oas_ragged(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), B, arr, erosion, dx,
+                                        _stream(stream), _ptr(R), ws.handle))
+
+
+def adjointSRKRagged(v, ux, uy, I, Gx_freq, Gy_freq, Ns, erosion, dx, stream, dLdI, dLdE, ws):
+    B, arr = _sizes(Ns)
+    _check(lib().srk_adjoint_ragged(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), B, arr,
+                                    erosion, dx, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
+
+
+def shrinkageTangentOaSRagged(f, g, df, dg, Gx_freq, Gy_freq, Ns, erosion, dx, stream, dh, ws):
+    B, arr = _sizes(Ns)
+    _check(lib().srk_tangent_ragged(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(Gx_freq), _ptr(Gy_freq), B, arr,
+                                    erosion, dx, _stream(stream), _ptr(dh), ws.handle))
+
+
+def shrinkageTangentAdjointOaSRagged(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_freq, Ns, erosion, dx, stream,
+                                     dLam_f, dLam_g, ws):
+    B, arr = _sizes(Ns)
+    _check(lib().srk_tangent_adjoint_ragged(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
+                                            _ptr(Gx_freq), _ptr(Gy_freq), B, arr, erosion, dx, _stream(stream),
+                                            _ptr(dLam_f), _ptr(dLam_g), ws.handle))
 
 
 def srkPrecomputeKernelFreq(K, kw, kh, M, G_freq, stream=None):

@@ -62,16 +62,31 @@ template <> struct OpTraits<OP_JVP>      { static constexpr int K = 1, L = 2; st
 template <> struct OpTraits<OP_TANADJ_F> { static constexpr int K = 1, L = 2; static constexpr bool PAIRS = false; };
 template <> struct OpTraits<OP_ADJ>      { static constexpr int K = 2, L = 1; static constexpr bool PAIRS = true; };
 
-// Tile geometry of one launch.
+// One image of a ragged batch: its size and where it starts in the
+// concatenated N-sized and W-sized batch arrays (elements).
+struct RagImage {
+  long long on, ow;
+  int N, W;
+  int blk0;  // first block of this image in the ragged stencil launch
+  int pad;
+};
+
+// Tile geometry of one launch.  A uniform batch tiles every image alike
+// (tile u -> image u / TT); a ragged batch of images of different N lists
+// its tiles in `rtile` (image, x0, y0) and its images in `rimg`.
 struct Geom {
   int M;      // FFT tile size
   int e;      // erosion (kernel half width bound)
   int S;      // valid outputs per tile per axis (<= M - 2e)
-  int T;      // tiles per axis
+  int T;      // tiles per axis (uniform batch)
   int Nin;    // virtual input size (N for forward-type, N + 2e for adjoint)
   int Wout;   // output size (W for forward-type, N for adjoint)
   int TT;     // T*T
-  int U;      // tiles in the whole batch (B*T*T)
+  int U;      // tiles in the whole batch
+  int N, W;   // image and valid-output size (uniform batch)
+  int wout_n; // outputs are N x N (adjoint-type) rather than W x W
+  const int4* __restrict__ rtile;      // ragged: tile -> (image, x0, y0, 0); else nullptr
+  const RagImage* __restrict__ rimg;   // ragged: per-image sizes and offsets
 };
 
 // Operand pointers.  All images are column-major; batch strides are
@@ -124,47 +139,59 @@ __device__ __forceinline__ float grad_y(const T* f, int N, int gx, int gy) {
 __device__ __forceinline__ float dot2(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
 
 struct TileRef {
-  int b, x0, y0;  // image index and tile origin in virtual input coordinates
+  int b, x0, y0;     // image index and tile origin in virtual input coordinates
   bool live;
+  int N, W, Wout;    // this image's size, valid-output size and output size
+  long long on, ow;  // offset of this image in N-sized / W-sized batch arrays
 };
 __device__ __forceinline__ TileRef tile_of(const Geom& g, int u) {
   TileRef t;
   t.live = u < g.U;
   const int uu = t.live ? u : 0;
-  t.b = uu / g.TT;
-  const int r = uu - t.b * g.TT;
-  const int tx = r / g.T, ty = r - (r / g.T) * g.T;
-  t.x0 = tx * g.S;
-  t.y0 = ty * g.S;
+  if (g.rtile) {
+    const int4 q = g.rtile[uu];
+    const RagImage im = g.rimg[q.x];
+    t.b = q.x;
+    t.x0 = q.y;
+    t.y0 = q.z;
+    t.N = im.N;
+    t.W = im.W;
+    t.on = im.on;
+    t.ow = im.ow;
+  } else {
+    t.b = uu / g.TT;
+    const int r = uu - t.b * g.TT;
+    const int tx = r / g.T, ty = r - (r / g.T) * g.T;
+    t.x0 = tx * g.S;
+    t.y0 = ty * g.S;
+    t.N = g.N;
+    t.W = g.W;
+    t.on = (long long)t.b * g.N * g.N;
+    t.ow = (long long)t.b * g.W * g.W;
+  }
+  t.Wout = g.wout_n ? t.N : t.W;
   return t;
 }
 
 // ---- loaders: value of field k of work tile w at local (x, y) ------------
-// Forward-type: image value of g at virtual coords (== image coords).
-template <typename T>
-__device__ __forceinline__ float img_at(const T* p, const OpArgs& a, int b, int gx, int gy) {
-  if (gx < 0 || gy < 0 || gx >= a.N || gy >= a.N) return 0.f;
-  return ldf(p, (long long)b * a.N * a.N + (long long)gx * a.N + gy);
-}
-
 // Adjoint-type: h_x = v*df/dx (or dv*df/dx + v*d(df)/dx for the
 // tangent-adjoint) on the valid window, zero elsewhere; virtual coords are
 // shifted by +e so that the full N x N output is the valid part of the
 // convolution of the zero-extended (N+2e)^2 field
 // (srk_adj_load_tile, adjoint/srk_adjoint.cuh:169-200).
 template <typename T>
-__device__ __forceinline__ float h_at(const OpArgs& a, int b, int k, int px, int py) {
+__device__ __forceinline__ float h_at(const OpArgs& a, const TileRef& t, int k, int px, int py) {
   const int qx = px - a.e, qy = py - a.e;            // image coords
   const int ox = qx - a.e, oy = qy - a.e;            // valid-window coords
-  if (ox < 0 || oy < 0 || ox >= a.W || oy >= a.W) return 0.f;
-  const long long vo = (long long)b * a.W * a.W + (long long)ox * a.W + oy;
-  const T* f = static_cast<const T*>(a.I) + (long long)b * a.N * a.N;
+  if (ox < 0 || oy < 0 || ox >= t.W || oy >= t.W) return 0.f;
+  const long long vo = t.ow + (long long)ox * t.W + oy;
+  const T* f = static_cast<const T*>(a.I) + t.on;
   const float v = ldf(static_cast<const T*>(a.v), vo);
-  const float g = (k == 0) ? grad_x(f, a.N, qx, qy) : grad_y(f, a.N, qx, qy);
+  const float g = (k == 0) ? grad_x(f, t.N, qx, qy) : grad_y(f, t.N, qx, qy);
   if (a.dI == nullptr) return v * g;
-  const T* df = static_cast<const T*>(a.dI) + (long long)b * a.N * a.N;
+  const T* df = static_cast<const T*>(a.dI) + t.on;
   const float dv = ldf(static_cast<const T*>(a.dv), vo);
-  const float dg = (k == 0) ? grad_x(df, a.N, qx, qy) : grad_y(df, a.N, qx, qy);
+  const float dg = (k == 0) ? grad_x(df, t.N, qx, qy) : grad_y(df, t.N, qx, qy);
   return dot2(dv, g, v, dg);
 }
 
@@ -173,17 +200,18 @@ __device__ __forceinline__ float h_at(const OpArgs& a, int b, int k, int px, int
 // loads are (base + immediate); bounds are tested per element only for a
 // tile that crosses the bottom edge.
 template <int M, typename T>
-__device__ __forceinline__ void load_tile_column(const T* __restrict__ img, int N, const TileRef& t, int x, int lane,
+__device__ __forceinline__ void load_tile_column(const T* __restrict__ img, const TileRef& t, int x, int lane,
                                                  float (&v)[M / tpf_of<M>()]) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
+  const int N = t.N;
   const int gx = t.x0 + x;
   if (!t.live || gx >= N) {
 #pragma unroll
     for (int i = 0; i < EPT; ++i) v[i] = 0.f;
     return;
   }
-  const T* col = img + (long long)t.b * N * N + (long long)gx * N + t.y0 + lane;
+  const T* col = img + t.on + (long long)gx * N + t.y0 + lane;
   const int rows = N - t.y0 - lane;  // rows available below this lane's first element
   if (N - t.y0 >= M) {
 #pragma unroll
@@ -204,22 +232,22 @@ __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int 
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       const int y = lane + TPF * i;
-      const float re = h_at<T>(a, t0.b, k, t0.x0 + x, t0.y0 + y);
-      const float im = t1.live ? h_at<T>(a, t1.b, k, t1.x0 + x, t1.y0 + y) : 0.f;
+      const float re = h_at<T>(a, t0, k, t0.x0 + x, t0.y0 + y);
+      const float im = t1.live ? h_at<T>(a, t1, k, t1.x0 + x, t1.y0 + y) : 0.f;
       z[i] = make_float2(re, im);
     }
   } else if constexpr (OpTraits<OP>::PAIRS) {
     float re[EPT], im[EPT];
     const T* E = static_cast<const T*>(a.E);
-    load_tile_column<M, T>(E, a.N, tile_of(g, 2 * w), x, lane, re);
-    load_tile_column<M, T>(E, a.N, tile_of(g, 2 * w + 1), x, lane, im);
+    load_tile_column<M, T>(E, tile_of(g, 2 * w), x, lane, re);
+    load_tile_column<M, T>(E, tile_of(g, 2 * w + 1), x, lane, im);
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z[i] = make_float2(re[i], im[i]);
   } else {
     float re[EPT], im[EPT];
     const TileRef t = tile_of(g, w);
-    load_tile_column<M, T>(static_cast<const T*>(a.E), a.N, t, x, lane, re);
-    load_tile_column<M, T>(static_cast<const T*>(a.dE), a.N, t, x, lane, im);
+    load_tile_column<M, T>(static_cast<const T*>(a.E), t, x, lane, re);
+    load_tile_column<M, T>(static_cast<const T*>(a.dE), t, x, lane, im);
 #pragma unroll
     for (int i = 0; i < EPT; ++i) z[i] = make_float2(re[i], im[i]);
   }
@@ -266,12 +294,12 @@ __device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int
 
 // Rows of this lane that carry valid outputs, as a bit mask over i.
 template <int M>
-__device__ __forceinline__ unsigned valid_rows(const Geom& g, int y0, int lane) {
+__device__ __forceinline__ unsigned valid_rows(const Geom& g, const TileRef& t, int lane) {
   unsigned m = 0;
 #pragma unroll
   for (int i = 0; i < M / tpf_of<M>(); ++i) {
     const int y = lane + tpf_of<M>() * i;
-    if (y >= g.e && y < g.e + g.S && y0 + y - g.e < g.Wout) m |= 1u << i;
+    if (y >= g.e && y < g.e + g.S && t.y0 + y - g.e < t.Wout) m |= 1u << i;
   }
   return m;
 }
@@ -281,16 +309,16 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
                                                 float2 (&z0)[M / tpf_of<M>()], float2 (&z1)[M / tpf_of<M>()]) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
-  const int N = a.N, W = a.W, e = a.e;
+  const int e = a.e;
   if constexpr (OP == OP_FWD || OP == OP_VJP_F) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const TileRef t = tile_of(g, 2 * w + h);
       const int ox = t.x0 + x - g.e;
-      if (!t.live || ox >= g.Wout) continue;
-      const unsigned vm = valid_rows<M>(g, t.y0, lane);
+      if (!t.live || ox >= t.Wout) continue;
+      const unsigned vm = valid_rows<M>(g, t, lane);
       // output row oy = y0 + y - e  ->  offset of row (y0 - e + lane)
-      const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+      const long long ob = t.ow + (long long)ox * t.W + t.y0 - g.e + lane;
       if constexpr (OP == OP_FWD) {
         T* __restrict__ R = static_cast<T*>(a.out0);
         T* __restrict__ UX = static_cast<T*>(a.out_ux);
@@ -306,8 +334,7 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
             if (vm >> i & 1u) stf(UY, ob + TPF * i, h ? z1[i].y : z1[i].x);
         }
         if (R) {
-          const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e,
-                                         t.y0 + lane, TPF);
+          const GradCol<T> gc = grad_col(static_cast<const T*>(a.I) + t.on, t.N, e, ox + e, t.y0 + lane, TPF);
           // gradients for all rows first (every load in flight before the
           // first store); the result overwrites this image's half of z0
 #pragma unroll
@@ -339,13 +366,13 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
   } else if constexpr (OP == OP_JVP || OP == OP_TANADJ_F) {
     const TileRef t = tile_of(g, w);
     const int ox = t.x0 + x - g.e;
-    if (ox >= g.Wout) return;
-    const unsigned vm = valid_rows<M>(g, t.y0, lane);
-    const long long ob = (long long)t.b * W * W + (long long)ox * W + t.y0 - g.e + lane;
+    if (ox >= t.Wout) return;
+    const unsigned vm = valid_rows<M>(g, t, lane);
+    const long long ob = t.ow + (long long)ox * t.W + t.y0 - g.e + lane;
     if constexpr (OP == OP_JVP) {
       // srk_tangent_combine (tan_tanadj/srk_tangent.cuh:28-52); re: conv of g, im: conv of dg
-      const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane, TPF);
-      const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + (long long)t.b * N * N, N, e, ox + e, t.y0 + lane, TPF);
+      const GradCol<T> gf = grad_col(static_cast<const T*>(a.I) + t.on, t.N, e, ox + e, t.y0 + lane, TPF);
+      const GradCol<T> gd = grad_col(static_cast<const T*>(a.dI) + t.on, t.N, e, ox + e, t.y0 + lane, TPF);
       T* __restrict__ DH = static_cast<T*>(a.out0);
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
@@ -368,8 +395,8 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
       for (int i = 0; i < EPT; ++i) {
         if (!(vm >> i & 1u)) continue;
         const float lam = ldf(LAM, ob + TPF * i), dlam = ldf(DLAM, ob + TPF * i);
-        WX[ob + TPF * i] = dlam * z0[i].x + lam * z0[i].y;
-        WY[ob + TPF * i] = dlam * z1[i].x + lam * z1[i].y;
+        WX[ob + TPF * i] = dot2(dlam, z0[i].x, lam, z0[i].y);
+        WY[ob + TPF * i] = dot2(dlam, z1[i].x, lam, z1[i].y);
       }
     }
   } else {  // OP_ADJ: output is the full N x N image
@@ -377,9 +404,9 @@ __device__ __forceinline__ void epilogue_column(const OpArgs& a, const Geom& g, 
     for (int h = 0; h < 2; ++h) {
       const TileRef t = tile_of(g, 2 * w + h);
       const int ox = t.x0 + x - g.e;
-      if (!t.live || ox >= g.Wout) continue;
-      const unsigned vm = valid_rows<M>(g, t.y0, lane);
-      const long long ob = (long long)t.b * N * N + (long long)ox * N + t.y0 - g.e + lane;
+      if (!t.live || ox >= t.Wout) continue;
+      const unsigned vm = valid_rows<M>(g, t, lane);
+      const long long ob = t.on + (long long)ox * t.N + t.y0 - g.e + lane;
       T* __restrict__ O = static_cast<T*>(a.out0);
 #pragma unroll
       for (int i = 0; i < EPT; ++i)
@@ -498,15 +525,15 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int RSP = TPF + TPF / 16;
-  const int W = a.W;
+  const int W = tr.W;
   const int rb = gw.off + t - g.e + 1;        // window row of element 0: y - e + 1, y = t
   const float* cm = win + line * gw.HP + rb;  // image column gx - 1
   const float* cc = cm + gw.HP;               // gx
   const float* cp = cc + gw.HP;               // gx + 1
   const int ox = tr.x0 + x - g.e;
-  if (!tr.live || ox >= g.Wout) return;
-  const unsigned vm = valid_rows<M>(g, tr.y0, t);
-  const long long ob = (long long)tr.b * W * W + (long long)ox * W + tr.y0 - g.e + t;
+  if (!tr.live || ox >= tr.Wout) return;
+  const unsigned vm = valid_rows<M>(g, tr, t);
+  const long long ob = tr.ow + (long long)ox * W + tr.y0 - g.e + t;
   if constexpr (OP == OP_FWD) {
     T* __restrict__ R = static_cast<T*>(a.out0);
     T* __restrict__ UX = static_cast<T*>(a.out_ux);
@@ -743,15 +770,18 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   };
   auto tile_h = [&](int h) { return tile_of(g, OP == OP_FWD ? 2 * w + h : w); };
   auto image_h = [&](int h) { return static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI); };
-  // 16-byte window copies: N % 4 == 0 and 16-byte aligned images
-  const bool vec16 = ASYNC && (a.N & 3) == 0 && (reinterpret_cast<uintptr_t>(a.I) & 15) == 0 &&
-                     (OP != OP_JVP || (reinterpret_cast<uintptr_t>(a.dI) & 15) == 0);
+  // 16-byte window copies: N % 4 == 0, a 16-byte aligned image start
+  auto vec16_of = [&](int h, const TileRef& tr) {
+    return ASYNC && (tr.N & 3) == 0 &&
+           ((reinterpret_cast<uintptr_t>(image_h(h)) + sizeof(float) * (uintptr_t)tr.on) & 15) == 0;
+  };
   auto issue_window = [&](int h, float* dst) {
     if constexpr (ASYNC) {
       const TileRef tr = tile_h(h);
+      const bool vec16 = vec16_of(h, tr);
       if (tr.live)
-        stage_grad_window_async(reinterpret_cast<const float*>(image_h(h)) + (long long)tr.b * a.N * a.N, a.N,
-                                window_of(h, tr, vec16), vec16, dst);
+        stage_grad_window_async(reinterpret_cast<const float*>(image_h(h)) + tr.on, tr.N, window_of(h, tr, vec16),
+                                vec16, dst);
       cp_async_commit();
     }
   };
@@ -791,11 +821,13 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
       cp_async_wait<1>();
       __syncthreads();
       const TileRef tr0 = tile_h(0);
-      if (active) epilogue_staged<M, OP, T>(a, g, tr0, xv + g.e, line, t, 0, z0s, z1, win0, window_of(0, tr0, vec16));
+      if (active)
+        epilogue_staged<M, OP, T>(a, g, tr0, xv + g.e, line, t, 0, z0s, z1, win0, window_of(0, tr0, vec16_of(0, tr0)));
       cp_async_wait<0>();
       __syncthreads();
       const TileRef tr1 = tile_h(1);
-      if (active) epilogue_staged<M, OP, T>(a, g, tr1, xv + g.e, line, t, 1, z0s, z1, win1, window_of(1, tr1, vec16));
+      if (active)
+        epilogue_staged<M, OP, T>(a, g, tr1, xv + g.e, line, t, 1, z0s, z1, win1, window_of(1, tr1, vec16_of(1, tr1)));
       return;
     }
   }
@@ -809,7 +841,7 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
         __syncthreads();  // rows of field 1 no longer used (round 0) / window consumed (round 1)
         const TileRef tr = tile_h(h);
         const GradWin gw = window_of(h, tr, false);
-        if (tr.live) stage_grad_window<T>(image_h(h) + (long long)tr.b * a.N * a.N, a.N, gw, win);
+        if (tr.live) stage_grad_window<T>(image_h(h) + tr.on, tr.N, gw, win);
         __syncthreads();
         if (active) epilogue_staged<M, OP, T>(a, g, tr, xv + g.e, line, t, h, z0s, z1, win, gw);
       }
@@ -1014,18 +1046,56 @@ __global__ void k_adj_wrt_f(const float* __restrict__ wx, const float* __restric
   auto WX = [&](int r, int c) -> float {
     if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
     const long long i = wb + (long long)c * W + r;
-    if constexpr (FROM_U) return ldf(ux, i) * ldf(v, i);
+    if constexpr (FROM_U) return __fmul_rn(ldf(ux, i), ldf(v, i));
     else return wx[i];
   };
   auto WY = [&](int r, int c) -> float {
     if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
     const long long i = wb + (long long)c * W + r;
-    if constexpr (FROM_U) return ldf(uy, i) * ldf(v, i);
+    if constexpr (FROM_U) return __fmul_rn(ldf(uy, i), ldf(v, i));
     else return wy[i];
   };
   const int ox = gx - e, oy = gy - e;
-  const float val = (WX(oy, ox - 1) - WX(oy, ox + 1)) * 0.5f + (WY(oy - 1, ox) - WY(oy + 1, ox)) * 0.5f;
+  const float val = __fadd_rn(__fmul_rn(__fsub_rn(WX(oy, ox - 1), WX(oy, ox + 1)), 0.5f),
+                             __fmul_rn(__fsub_rn(WY(oy - 1, ox), WY(oy + 1, ox)), 0.5f));
   stf(out, (long long)b * N * N + (long long)gx * N + gy, val);
+}
+
+// The same for a ragged batch: one 32 x 8 block per block of pixels, the
+// blocks of image b starting at rimg[b].blk0.
+template <typename T, bool FROM_U>
+__global__ void k_adj_wrt_f_rag(const float* __restrict__ wx, const float* __restrict__ wy, const T* __restrict__ v,
+                                const T* __restrict__ ux, const T* __restrict__ uy,
+                                const RagImage* __restrict__ rimg, int B, int e, T* __restrict__ out) {
+  int lo = 0, hi = B - 1;
+  const int blk = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rimg[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
+  }
+  const RagImage im = rimg[lo];
+  const int N = im.N, W = im.W;
+  const int nby = (N + 31) / 32;
+  const int k = blk - im.blk0;
+  const int gy = (k % nby) * 32 + threadIdx.x;
+  const int gx = (k / nby) * 8 + threadIdx.y;
+  if (gx >= N || gy >= N) return;
+  auto WX = [&](int r, int c) -> float {
+    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
+    const long long i = im.ow + (long long)c * W + r;
+    if constexpr (FROM_U) return __fmul_rn(ldf(ux, i), ldf(v, i));
+    else return wx[i];
+  };
+  auto WY = [&](int r, int c) -> float {
+    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
+    const long long i = im.ow + (long long)c * W + r;
+    if constexpr (FROM_U) return __fmul_rn(ldf(uy, i), ldf(v, i));
+    else return wy[i];
+  };
+  const int ox = gx - e, oy = gy - e;
+  const float val = __fadd_rn(__fmul_rn(__fsub_rn(WX(oy, ox - 1), WX(oy, ox + 1)), 0.5f),
+                             __fmul_rn(__fsub_rn(WY(oy - 1, ox), WY(oy + 1, ox)), 0.5f));
+  stf(out, im.on + (long long)gx * N + gy, val);
 }
 
 }  // namespace srk

@@ -77,6 +77,15 @@ struct srk_plan_s {
   unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
   int persist_lag = 0, persist_grid = 0, persist_prefetch = 0;
   int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
+  // ragged batches: device tables of the last ragged call (tile -> image,
+  // per-image sizes/offsets), rebuilt only when the image sizes change
+  int4* rag_tiles = nullptr;
+  size_t rag_tiles_cap = 0;
+  srk::RagImage* rag_imgs = nullptr;
+  size_t rag_imgs_cap = 0;
+  std::vector<int> rag_key;
+  int rag_ntiles_fwd = 0, rag_ntiles_adj = 0, rag_nblk = 0;
+  long long rag_sum_nn = 0, rag_sum_ww = 0;
 };
 
 namespace srk {

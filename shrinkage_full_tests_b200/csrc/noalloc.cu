@@ -143,6 +143,8 @@ extern "C" srk_status srk_training_forward_noalloc(const float* d_E, const float
   a.N = N; a.W = W; a.e = erosion;
   a.E = d_E; a.I = d_I; a.out0 = d_R;
   Geom g;
+  std::memset(&g, 0, sizeof(g));
   g.M = M; g.e = erosion; g.S = S; g.T = 1; g.Nin = N; g.Wout = W; g.TT = 1; g.U = B;
+  g.N = N; g.W = W;
   return launch_conv<OP_FWD, float>(&view, a, g, false, s);
 }

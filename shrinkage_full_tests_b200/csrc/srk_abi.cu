@@ -57,14 +57,18 @@ int choose_tile(int N, int W, int e) {
 
 Geom fwd_geom(const srk_plan_s* p, int B) {
   Geom g;
+  std::memset(&g, 0, sizeof(g));
   g.M = p->M; g.e = p->e; g.S = p->S; g.T = p->T;
   g.Nin = p->N; g.Wout = p->W; g.TT = p->T * p->T; g.U = B * g.TT;
+  g.N = p->N; g.W = p->W; g.wout_n = 0;
   return g;
 }
 Geom adj_geom(const srk_plan_s* p, int B) {
   Geom g;
+  std::memset(&g, 0, sizeof(g));
   g.M = p->M; g.e = p->e; g.S = p->S; g.T = p->Ta;
   g.Nin = p->N + 2 * p->e; g.Wout = p->N; g.TT = p->Ta * p->Ta; g.U = B * g.TT;
+  g.N = p->N; g.W = p->W; g.wout_n = 1;
   return g;
 }
 
@@ -415,6 +419,8 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->G[1]) cudaFree(p->G[1]);
   if (p->tw) cudaFree(p->tw);
   if (p->wbuf) cudaFree(p->wbuf);
+  if (p->rag_tiles) cudaFree(p->rag_tiles);
+  if (p->rag_imgs) cudaFree(p->rag_imgs);
   if (p->ctl) cudaFree(p->ctl);
   if (p->mailbox) cudaFreeHost(p->mailbox);
   if (p->mailbox_spins) cudaFreeHost(p->mailbox_spins);
@@ -672,6 +678,186 @@ srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, 
   return launch_conv_dt<OP_JVP>(p, a, fwd_geom(p, B), false, s);
 }
 
+// ---- ragged batches -----------------------------------------------------------
+// B images of sizes Ns[b] (each 2*erosion+1 <= N_b <= the plan's N; same
+// erosion, dx, tile size and spectra), concatenated column-major in every
+// buffer: N-sized arrays hold N_b^2 elements per image, W-sized ones W_b^2.
+// The tile tables of the forward-type (valid W_b outputs) and adjoint-type
+// (N_b outputs) geometries are built together and uploaded once per
+// distinct Ns; calls with new sizes re-upload them in stream order.
+srk_status ragged_tables(srk_plan_s* p, int B, const int* Ns, cudaStream_t s) {
+  if (B < 1) return fail(SRK_ERR_INVALID_ARG, "ragged batch needs B >= 1 (got %d)", B);
+  if (!Ns) return fail(SRK_ERR_INVALID_ARG, "Ns is NULL");
+  const int e = p->e, S = p->S;
+  std::vector<int> key(Ns, Ns + B);
+  for (int b = 0; b < B; ++b)
+    if (Ns[b] < 2 * e + 1 || Ns[b] > p->N)
+      return fail(SRK_ERR_INVALID_ARG, "image %d: N=%d outside [2*erosion+1=%d, plan N=%d]", b, Ns[b], 2 * e + 1, p->N);
+  if (key == p->rag_key) return SRK_OK;
+  std::vector<int4> fwd, adj;
+  std::vector<RagImage> imgs(B);
+  long long on = 0, ow = 0, blk = 0;
+  for (int b = 0; b < B; ++b) {
+    const int N = Ns[b], W = N - 2 * e;
+    imgs[b].on = on;
+    imgs[b].ow = ow;
+    imgs[b].N = N;
+    imgs[b].W = W;
+    imgs[b].blk0 = (int)blk;
+    imgs[b].pad = 0;
+    on += (long long)N * N;
+    ow += (long long)W * W;
+    blk += (long long)((N + 31) / 32) * ((N + 7) / 8);
+    const int Tf = (W + S - 1) / S, Ta = (N + S - 1) / S;
+    for (int tx = 0; tx < Tf; ++tx)
+      for (int ty = 0; ty < Tf; ++ty) fwd.push_back(make_int4(b, tx * S, ty * S, 0));
+    for (int tx = 0; tx < Ta; ++tx)
+      for (int ty = 0; ty < Ta; ++ty) adj.push_back(make_int4(b, tx * S, ty * S, 0));
+  }
+  if (blk > (1ll << 30) || fwd.size() + adj.size() > (1u << 30))
+    return fail(SRK_ERR_UNSUPPORTED, "ragged batch too large (%lld pixel blocks)", blk);
+  const size_t nt = fwd.size() + adj.size();
+  if (p->rag_tiles_cap < nt) {
+    if (p->rag_tiles) SRK_CUDA(cudaFreeAsync(p->rag_tiles, s));
+    p->rag_tiles = nullptr;
+    p->rag_tiles_cap = 0;
+    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_tiles), nt * sizeof(int4), s));
+    p->rag_tiles_cap = nt;
+  }
+  if (p->rag_imgs_cap < (size_t)B) {
+    if (p->rag_imgs) SRK_CUDA(cudaFreeAsync(p->rag_imgs, s));
+    p->rag_imgs = nullptr;
+    p->rag_imgs_cap = 0;
+    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_imgs), (size_t)B * sizeof(RagImage), s));
+    p->rag_imgs_cap = B;
+  }
+  fwd.insert(fwd.end(), adj.begin(), adj.end());
+  // pageable sources: the copies have taken the data when the calls return
+  SRK_CUDA(cudaMemcpyAsync(p->rag_tiles, fwd.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, s));
+  SRK_CUDA(cudaMemcpyAsync(p->rag_imgs, imgs.data(), (size_t)B * sizeof(RagImage), cudaMemcpyHostToDevice, s));
+  p->rag_key = key;
+  p->rag_ntiles_fwd = (int)(nt - adj.size());
+  p->rag_ntiles_adj = (int)adj.size();
+  p->rag_nblk = (int)blk;
+  p->rag_sum_nn = on;
+  p->rag_sum_ww = ow;
+  return SRK_OK;
+}
+
+Geom ragged_geom(const srk_plan_s* p, bool adj) {
+  Geom g = adj ? adj_geom(p, 1) : fwd_geom(p, 1);
+  g.U = adj ? p->rag_ntiles_adj : p->rag_ntiles_fwd;
+  g.rtile = p->rag_tiles + (adj ? p->rag_ntiles_fwd : 0);
+  g.rimg = p->rag_imgs;
+  return g;
+}
+
+template <typename T>
+void adj_wrt_f_rag_t(srk_plan_s* p, const float* wx, const float* wy, const void* v, const void* ux, const void* uy,
+                     int B, void* out, cudaStream_t s) {
+  const dim3 blk(32, 8);
+  if (ux)
+    k_adj_wrt_f_rag<T, true><<<p->rag_nblk, blk, 0, s>>>(nullptr, nullptr, static_cast<const T*>(v),
+                                                         static_cast<const T*>(ux), static_cast<const T*>(uy),
+                                                         p->rag_imgs, B, p->e, static_cast<T*>(out));
+  else
+    k_adj_wrt_f_rag<T, false><<<p->rag_nblk, blk, 0, s>>>(wx, wy, nullptr, nullptr, nullptr, p->rag_imgs, B, p->e,
+                                                          static_cast<T*>(out));
+}
+
+srk_status adj_wrt_f_rag(srk_plan_s* p, const float* wx, const float* wy, const void* v, const void* ux,
+                         const void* uy, int B, void* out, cudaStream_t s) {
+  switch (p->dtype) {
+    case SRK_F32: adj_wrt_f_rag_t<float>(p, wx, wy, v, ux, uy, B, out, s); break;
+    case SRK_F16: adj_wrt_f_rag_t<__half>(p, wx, wy, v, ux, uy, B, out, s); break;
+    case SRK_BF16: adj_wrt_f_rag_t<__nv_bfloat16>(p, wx, wy, v, ux, uy, B, out, s); break;
+  }
+  return cuda_status(cudaGetLastError(), "ragged adj_wrt_f launch");
+}
+
+srk_status check_ragged(const srk_plan_s* p, int erosion, float dx) {
+  if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
+  if (erosion != p->e) return fail(SRK_ERR_INVALID_ARG, "erosion=%d differs from the plan's %d", erosion, p->e);
+  if (dx != p->dx) return fail(SRK_ERR_INVALID_ARG, "dx=%g differs from the plan's dx=%g", dx, p->dx);
+  return SRK_OK;
+}
+
+srk_status op_forward_oas_ragged(const void* E, const void* I, const void* gx, const void* gy, int B, const int* Ns,
+                                 int erosion, float dx, srk_stream_t s, void* R, srk_plan p) {
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(E);
+  SRK_NONNULL(I);
+  SRK_NONNULL(R);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(ragged_tables(p, B, Ns, s));
+  OpArgs a = base_args(p);
+  a.E = E; a.I = I; a.out0 = R;
+  return launch_conv_dt<OP_FWD>(p, a, ragged_geom(p, false), false, s);
+}
+
+srk_status op_adjoint_ragged(const void* v, const void* ux, const void* uy, const void* I, const void* gx,
+                             const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s, void* dLdI,
+                             void* dLdE, srk_plan p) {
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(v);
+  SRK_NONNULL(ux);
+  SRK_NONNULL(uy);
+  SRK_NONNULL(I);
+  SRK_NONNULL(dLdI);
+  SRK_NONNULL(dLdE);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(ragged_tables(p, B, Ns, s));
+  SRK_TRY(adj_wrt_f_rag(p, nullptr, nullptr, v, ux, uy, B, dLdI, s));
+  OpArgs a = base_args(p);
+  a.v = v; a.I = I; a.out0 = dLdE;
+  return launch_conv_dt<OP_ADJ>(p, a, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
+}
+
+srk_status op_tangent_ragged(const void* f, const void* g, const void* df, const void* dg, const void* gx,
+                             const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s, void* dh,
+                             srk_plan p) {
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(f);
+  SRK_NONNULL(g);
+  SRK_NONNULL(df);
+  SRK_NONNULL(dg);
+  SRK_NONNULL(dh);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(ragged_tables(p, B, Ns, s));
+  OpArgs a = base_args(p);
+  a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
+  return launch_conv_dt<OP_JVP>(p, a, ragged_geom(p, false), false, s);
+}
+
+srk_status op_tangent_adjoint_ragged(const void* f, const void* g, const void* df, const void* dg, const void* lam,
+                                     const void* dlam, const void* gx, const void* gy, int B, const int* Ns,
+                                     int erosion, float dx, srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(f);
+  SRK_NONNULL(g);
+  SRK_NONNULL(df);
+  SRK_NONNULL(dg);
+  SRK_NONNULL(lam);
+  SRK_NONNULL(dlam);
+  SRK_NONNULL(dLam_f);
+  SRK_NONNULL(dLam_g);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(ragged_tables(p, B, Ns, s));
+  const size_t ww = (size_t)p->rag_sum_ww;
+  SRK_TRY(ensure_wbuf(p, 2 * ww * sizeof(float), s));
+  OpArgs a = base_args(p);
+  a.E = g; a.dE = dg; a.v = lam; a.dv = dlam; a.out0 = p->wbuf; a.out1 = p->wbuf + ww;
+  SRK_TRY(launch_conv_dt<OP_TANADJ_F>(p, a, ragged_geom(p, false), false, s));
+  SRK_TRY(adj_wrt_f_rag(p, p->wbuf, p->wbuf + ww, nullptr, nullptr, nullptr, B, dLam_f, s));
+  OpArgs b = base_args(p);
+  b.v = lam; b.dv = dlam; b.I = f; b.dI = df; b.out0 = dLam_g;
+  return launch_conv_dt<OP_ADJ>(p, b, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
+}
+
 // The float* entry points are the reference drop-ins: fp32 plans only.
 srk_status need_f32(srk_plan p) {
   if (p && p->dtype != SRK_F32)
@@ -736,6 +922,34 @@ srk_status srk_jvp(const float* f, const float* g, const float* df, const float*
                    float* dh, srk_plan p) {
   SRK_TRY(need_f32(p));
   return op_jvp(f, g, df, dg, B, s, dh, p);
+}
+
+srk_status srk_forward_oas_ragged(const float* E, const float* I, const void* gx, const void* gy, int B,
+                                  const int* Ns, int erosion, float dx, srk_stream_t s, float* R, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_forward_oas_ragged(E, I, gx, gy, B, Ns, erosion, dx, s, R, p);
+}
+
+srk_status srk_adjoint_ragged(const float* v, const float* ux, const float* uy, const float* I, const void* gx,
+                              const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s,
+                              float* dLdI, float* dLdE, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_adjoint_ragged(v, ux, uy, I, gx, gy, B, Ns, erosion, dx, s, dLdI, dLdE, p);
+}
+
+srk_status srk_tangent_ragged(const float* f, const float* g, const float* df, const float* dg, const void* gx,
+                              const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s, float* dh,
+                              srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent_ragged(f, g, df, dg, gx, gy, B, Ns, erosion, dx, s, dh, p);
+}
+
+srk_status srk_tangent_adjoint_ragged(const float* f, const float* g, const float* df, const float* dg,
+                                      const float* lam, const float* dlam, const void* gx, const void* gy, int B,
+                                      const int* Ns, int erosion, float dx, srk_stream_t s, float* dLam_f,
+                                      float* dLam_g, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent_adjoint_ragged(f, g, df, dg, lam, dlam, gx, gy, B, Ns, erosion, dx, s, dLam_f, dLam_g, p);
 }
 
 // ---- storage-typed forms: element type of every image buffer = plan dtype ------
