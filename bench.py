@@ -129,20 +129,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def grf_batch(torch, B, N, seed0, ell=8.0, chunk=250):
-    """Seeded Gaussian random fields on the device, col-major [B][N][N]."""
+def grf_batch(torch, B, N, seed0, ell=8.0):
+    """Seeded Gaussian random fields generated on the device by the library
+    (srk_grf: Philox noise, GpGenerator's filter, min-max scaled), [B][N][N]."""
+    import shrinkage_full_tests_b200 as srk
     out = torch.empty((B, N, N), device="cuda", dtype=torch.float32)
-    k = torch.fft.fftfreq(N, device="cuda", dtype=torch.float64)
-    H = torch.exp(-2.0 * (torch.pi ** 2) * ell ** 2 * (k[:, None] ** 2 + k[None, :] ** 2))
-    for b0 in range(0, B, chunk):
-        b1 = min(B, b0 + chunk)
-        gen = torch.Generator(device="cuda")
-        gen.manual_seed(seed0 + b0)
-        w = torch.randn((b1 - b0, N, N), device="cuda", dtype=torch.float64, generator=gen)
-        x = torch.fft.ifft2(torch.fft.fft2(w) * H).real
-        mn = x.amin(dim=(1, 2), keepdim=True)
-        mx = x.amax(dim=(1, 2), keepdim=True)
-        out[b0:b1] = ((x - mn) / (mx - mn)).float()
+    srk.grf(out, ell, seed0)
+    torch.cuda.synchronize()
     return out
 
 

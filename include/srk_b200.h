@@ -211,6 +211,24 @@ srk_status srk_tangent_adjoint_ragged(const float* d_f, const float* d_g, const 
                                       const void* d_Gy_freq, int B, const int* Ns, int erosion, float dx,
                                       srk_stream_t stream, float* d_dLam_f, float* d_dLam_g, srk_plan plan);
 
+/* ---- synthetic inputs on the device -----------------------------------------
+ * Gaussian random fields as GpGenerator (third_party/include/stTestCore/
+ * gp_generator.h:95-254): white N(0,1) noise on the Np x Np grid (Np = next
+ * power of two >= N) filtered by sqrt(FFT2(c)) of the periodic covariance
+ * c(r) = exp(-r^2 / (2 ell^2)), cropped to the top-left N x N; d_out
+ * [B][N][N].  minmax = 1 scales every image to [0, 1].  srk_grf draws the
+ * noise with Philox4x32-10 keyed by seed + b (image b does not depend on B);
+ * srk_grf_filter takes caller noise [B][Np][Np] (column-major) instead. */
+srk_status srk_grf(int B, int N, double ell, unsigned long long seed, int minmax, srk_stream_t stream,
+                   float* d_out);
+srk_status srk_grf_filter(const float* d_noise, int B, int N, double ell, int minmax, srk_stream_t stream,
+                          float* d_out);
+/* Line/space patterns as gen_lns_vertical / gen_lns_horizontal
+ * (third_party/src/patternUtil/test_pattern.cu:83-109): kinds is a HOST
+ * array of B entries, 0 = vertical lines, 1 = horizontal; period_px 0 = 4 FWHM. */
+srk_status srk_lns(int B, int N, const int* kinds, float sigma_px, float period_px, int num_nbrs,
+                   srk_stream_t stream, float* d_out);
+
 /* ---- critical dimension (CD) of line/space signals ------------------------
  * MeasureCD_Batched (third_party/src/metricUtil/cd_measure_util.cu:310-437)
  * in one kernel per signal: L-fold windowed-sinc upsampling (half width A),

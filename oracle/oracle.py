@@ -174,18 +174,75 @@ def kernel_freq(K, M):
     return out
 
 
+def next_pow2(n):
+    p = 1
+    while p < n:
+        p <<= 1
+    return p
+
+
+def grf_filter(noise, N, ell):
+    """Filter white noise (Np, Np) [col, row] as GpGenerator::generate
+    (third_party/include/stTestCore/gp_generator.h:119-147, filter :180-201):
+    H = sqrt(max(0, Re FFT2(c))) of the periodic covariance
+    c(dx, dy) = exp(-(dx^2 + dy^2) / (2 ell^2)) with nearest-image
+    displacements d in (-Np/2, Np/2], x = Re IFFT2(H FFT2(w)), cropped to
+    the top-left N x N.  FP64."""
+    w = np.asarray(noise, np.float64)
+    Np = w.shape[0]
+    d = np.arange(Np)
+    d = np.where(d <= Np // 2, d, d - Np).astype(np.float64)
+    c = np.exp(-0.5 * (d[:, None] ** 2 + d[None, :] ** 2) / (ell * ell))
+    H = np.sqrt(np.maximum(0.0, np.fft.fft2(c).real))
+    x = np.fft.ifft2(H * np.fft.fft2(w)).real
+    return x[:N, :N]
+
+
+def minmax01(x):
+    return (x - x.min()) / (x.max() - x.min())
+
+
 def grf(N, ell, seed):
     """Seeded Gaussian random field, col-major (N, N) float32: white N(0,1)
-    noise (numpy PCG64, this seed) filtered periodically by exp(-r^2/2 ell^2),
-    then min-max scaled to [0, 1]."""
-    rng = np.random.default_rng(seed)
-    w = rng.standard_normal((N, N))
-    k = np.fft.fftfreq(N)
-    kk = k[:, None] ** 2 + k[None, :] ** 2
-    H = np.exp(-2.0 * (np.pi ** 2) * (ell ** 2) * kk)
-    x = np.fft.ifft2(np.fft.fft2(w) * H).real
-    x = (x - x.min()) / (x.max() - x.min())
-    return x.astype(np.float32)
+    noise (numpy PCG64, this seed) on the padded grid, filtered as
+    GpGenerator (grf_filter), then min-max scaled to [0, 1]."""
+    Np = next_pow2(N)
+    w = np.random.default_rng(seed).standard_normal((Np, Np))
+    return minmax01(grf_filter(w, N, ell)).astype(np.float32)
+
+
+# ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC 2011), vectorised
+_PH_M0, _PH_M1, _PH_W0, _PH_W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+
+
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Counters c0..c3 (uint32 arrays or ints), key (k0, k1): the 4 output words."""
+    m32 = np.uint64(0xFFFFFFFF)
+    c = [np.asarray(v, np.uint64) & m32 for v in (c0, c1, c2, c3)]
+    k = [np.uint64(k0 & 0xFFFFFFFF), np.uint64(k1 & 0xFFFFFFFF)]
+    for r in range(10):
+        if r:
+            k = [(k[0] + np.uint64(_PH_W0)) & m32, (k[1] + np.uint64(_PH_W1)) & m32]
+        p0 = np.uint64(_PH_M0) * c[0]
+        p1 = np.uint64(_PH_M1) * c[2]
+        c = [(p1 >> np.uint64(32)) ^ c[1] ^ k[0], p1 & m32, (p0 >> np.uint64(32)) ^ c[3] ^ k[1], p0 & m32]
+    return [v.astype(np.uint32) for v in c]
+
+
+def philox_noise(N, seed, b=0):
+    """The white noise of the device generator for image b (key seed + b):
+    (Np, Np) [col, row]; pixel p = col*Np + row takes word p mod 4 of the
+    Philox block p // 4, pairs (0,1), (2,3) through Box-Muller, uniforms
+    (bits + 0.5) 2^-32.  Float32 like the device."""
+    Np = next_pow2(N)
+    q = np.arange(Np * Np // 4, dtype=np.uint64)
+    key = (seed + b) & 0xFFFFFFFFFFFFFFFF
+    r = philox4x32_10(q & np.uint64(0xFFFFFFFF), q >> np.uint64(32), 0, 0, key & 0xFFFFFFFF, key >> 32)
+    u = [((v.astype(np.float32) + np.float32(0.5)) * np.float32(2.0 ** -32)).astype(np.float64) for v in r]
+    m0, m1 = np.sqrt(-2.0 * np.log(u[0])), np.sqrt(-2.0 * np.log(u[2]))
+    a0, a1 = 2.0 * np.pi * u[1], 2.0 * np.pi * u[3]
+    z = np.stack([m0 * np.cos(a0), m0 * np.sin(a0), m1 * np.cos(a1), m1 * np.sin(a1)], axis=1).ravel()
+    return z.reshape(Np, Np)
 
 
 def ref_host():
@@ -198,6 +255,7 @@ def ref_host():
         L = ctypes.CDLL(path)
         L.ref_gp_field.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong, _fp]
         L.ref_lns.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, _fp]
+        L.ref_gp_noise.argtypes = [ctypes.c_int, ctypes.c_ulonglong, _dp]
         _ref_host = L
     return _ref_host
 
@@ -206,6 +264,14 @@ def ref_gp_field(N, ell, seed):
     """GpGenerator(Covariance2D::isotropic(ell), N, N, seed).generate()."""
     out = np.empty((N, N), np.float32)
     ref_host().ref_gp_field(N, ell, seed, out.ctypes.data_as(_fp))
+    return out
+
+
+def ref_gp_noise(N, seed):
+    """The white noise GpGenerator draws for this seed, (Np, Np) [col, row]."""
+    Np = next_pow2(N)
+    out = np.empty((Np, Np), np.float64)
+    ref_host().ref_gp_noise(N, seed, out.ctypes.data_as(_dp))
     return out
 
 

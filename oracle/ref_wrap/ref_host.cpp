@@ -6,12 +6,27 @@
 #include <stTestCore/gp_generator.h>
 #include <patternUtil/test_pattern.h>
 #include <cstring>
+#include <random>
 
 extern "C" int ref_gp_field(int N, double ell, unsigned long long seed, float* out) {
   st::util::GpGenerator g(st::util::Covariance2D::isotropic(ell), N, N, seed);
   const std::vector<float> v = g.generate();
   std::memcpy(out, v.data(), sizeof(float) * v.size());
   return (int)v.size();
+}
+
+// The white noise GpGenerator::generate draws for this seed (the same
+// engine, distribution and order: one std::normal_distribution per call,
+// row-major over the padded Np x Np grid), written column-major
+// out[c*Np + r], so that filtering it reproduces ref_gp_field.  Returns Np.
+extern "C" int ref_gp_noise(int N, unsigned long long seed, double* out) {
+  int Np = 1;
+  while (Np < N) Np <<= 1;
+  std::mt19937_64 rng(static_cast<std::mt19937_64::result_type>(seed));
+  std::normal_distribution<double> normal(0.0, 1.0);
+  for (int r = 0; r < Np; ++r)
+    for (int c = 0; c < Np; ++c) out[(size_t)c * Np + r] = normal(rng);
+  return Np;
 }
 
 // kind: 0 = LNS vertical, 1 = LNS horizontal.  period 0 = auto (4 FWHM).

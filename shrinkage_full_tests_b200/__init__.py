@@ -86,6 +86,9 @@ _SIGS = {
     "srk_forward": [_P, _P, _I, _P, _P, _P],
     "srk_vjp": [_P, _P, _P, _I, _P, _P, _P, _P],
     "srk_jvp": [_P, _P, _P, _P, _I, _P, _P, _P],
+    "srk_grf": [_I, _I, _D, ctypes.c_ulonglong, _I, _P, _P],
+    "srk_grf_filter": [_P, _I, _I, _D, _I, _P, _P],
+    "srk_lns": [_I, _I, _P, _F, _F, _I, _P, _P],
     "srk_forward_oas_ragged": [_P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P],
     "srk_adjoint_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P, _P],
     "srk_tangent_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P],
@@ -270,6 +273,27 @@ def shrinkageTangentAdjointOaSRagged(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_fr
     _check(lib().srk_tangent_adjoint_ragged(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
                                             _ptr(Gx_freq), _ptr(Gy_freq), B, arr, erosion, dx, _stream(stream),
                                             _ptr(dLam_f), _ptr(dLam_g), ws.handle))
+
+
+# ---- synthetic inputs on the device
+def grf(out, ell, seed, minmax=True, stream=None):
+    """Gaussian random fields into out [B][N][N] (float32, CUDA): image b is
+    keyed by seed + b."""
+    B, N = (1, out.shape[-1]) if out.dim() == 2 else (out.shape[0], out.shape[-1])
+    _check(lib().srk_grf(B, N, float(ell), int(seed), 1 if minmax else 0, _stream(stream), _ptr(out)))
+
+
+def grf_filter(noise, out, ell, minmax=False, stream=None):
+    """Filter caller noise [B][Np][Np] into out [B][N][N]."""
+    B, N = (1, out.shape[-1]) if out.dim() == 2 else (out.shape[0], out.shape[-1])
+    _check(lib().srk_grf_filter(_ptr(noise), B, N, float(ell), 1 if minmax else 0, _stream(stream), _ptr(out)))
+
+
+def lns(out, kinds, sigma_px, period_px=0.0, num_nbrs=4, stream=None):
+    """Line/space patterns into out [B][N][N]; kinds[b] 0 = vertical, 1 = horizontal."""
+    B, arr = _sizes(kinds)
+    _check(lib().srk_lns(B, out.shape[-1], arr, float(sigma_px), float(period_px), num_nbrs, _stream(stream),
+                         _ptr(out)))
 
 
 def srkPrecomputeKernelFreq(K, kw, kh, M, G_freq, stream=None):

@@ -123,3 +123,34 @@ def test_windowed_forward_matches_full():
     full = O.forward(E, I, Kx, Ky, e, 1.0)
     win = O.forward(E, I, Kx, Ky, e, 1.0, window=(5, 9, 20, 13))
     assert np.array_equal(win, full[5:25, 9:22])
+
+
+def test_philox_known_answers():
+    """Philox4x32-10 known-answer vectors of the published algorithm
+    (Salmon et al., SC 2011; Random123 test vectors)."""
+    m = 0xFFFFFFFF
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+             ((m, m, m, m), (m, m), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+             ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+              (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1))]
+    for c, k, want in cases:
+        got = O.philox4x32_10(*c, *k)
+        assert tuple(int(v) for v in got) == want
+
+
+def test_philox_noise_is_standard_normal():
+    z = O.philox_noise(256, 1234)
+    assert abs(z.mean()) < 0.01 and abs(z.var() - 1.0) < 0.01
+    # neighbouring pixels uncorrelated
+    assert abs(np.mean(z[:, 1:] * z[:, :-1])) < 0.01
+    assert abs(np.mean(z[1:, :] * z[:-1, :])) < 0.01
+
+
+@pytest.mark.skipif(O.ref_host() is None, reason="reference generators not built")
+@pytest.mark.parametrize("N,ell,seed", [(64, 8.0, 7), (50, 8.0, 11), (96, 3.0, 5)])
+def test_grf_filter_reproduces_reference_generator(N, ell, seed):
+    """Given GpGenerator's own noise, the oracle's filter reproduces its field
+    (gp_generator.h:119-147) to the float rounding of its output."""
+    ref = O.ref_gp_field(N, ell, seed).astype(np.float64)
+    ours = O.grf_filter(O.ref_gp_noise(N, seed), N, ell)
+    assert np.abs(ours - ref).max() < 1e-6 * np.abs(ref).max()
