@@ -159,11 +159,17 @@ __device__ __forceinline__ TileRef tile_of(const Geom& g, int u) {
     t.on = im.on;
     t.ow = im.ow;
   } else {
-    t.b = uu / g.TT;
-    const int r = uu - t.b * g.TT;
-    const int tx = r / g.T, ty = r - (r / g.T) * g.T;
-    t.x0 = tx * g.S;
-    t.y0 = ty * g.S;
+    if (g.TT == 1) {  // one tile per image (tile size >= image): no divisions
+      t.b = uu;
+      t.x0 = 0;
+      t.y0 = 0;
+    } else {
+      t.b = uu / g.TT;
+      const int r = uu - t.b * g.TT;
+      const int tx = r / g.T, ty = r - (r / g.T) * g.T;
+      t.x0 = tx * g.S;
+      t.y0 = ty * g.S;
+    }
     t.N = g.N;
     t.W = g.W;
     t.on = (long long)t.b * g.N * g.N;

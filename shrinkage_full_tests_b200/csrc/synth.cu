@@ -216,17 +216,23 @@ int grf_taps(int Np, double ell, std::vector<float>& hzp, std::vector<float>& hz
   const int D = std::min(Np / 2, (int)std::ceil(12.0 * ell));
   std::vector<double> c(D + 1);
   for (int d = 0; d <= D; ++d) c[d] = std::exp(-0.5 * (double)d * d / (ell * ell));
-  std::vector<double> Hp(Np / 2 + 1), Hn(Np / 2 + 1);
-  bool neg = false;
+  std::vector<double> S(Np / 2 + 1), Hp(Np / 2 + 1), Hn(Np / 2 + 1);
   for (int k = 0; k <= Np / 2; ++k) {
     double s = c[0];
     for (int d = 1; d <= D; ++d) {
       const double term = c[d] * ct[(long long)k * d % Np];
       s += (2 * d == Np) ? term : 2.0 * term;  // d = Np/2 occurs once
     }
-    Hp[k] = std::sqrt(std::max(0.0, s));
-    Hn[k] = std::sqrt(std::max(0.0, -s));
-    neg = neg || s < 0.0;
+    S[k] = s;
+  }
+  // negative values at the level of the summation's rounding are zeros
+  // (their products in the 2-D filter are below 1e-24 of its peak)
+  const double floor_s = 1e-12 * S[0];
+  bool neg = false;
+  for (int k = 0; k <= Np / 2; ++k) {
+    Hp[k] = std::sqrt(std::max(0.0, S[k]));
+    Hn[k] = S[k] < -floor_s ? std::sqrt(-S[k]) : 0.0;
+    neg = neg || S[k] < -floor_s;
   }
   // h(d) = (1/Np) sum_k H(k) e^{2 pi i k d / Np}, H even in k
   auto h_at = [&](const std::vector<double>& H, int d) {

@@ -71,3 +71,17 @@ def test_lns_matches_reference_generator(torch_cuda):
     for b, k in enumerate(kinds):
         ref = O.ref_lns(k == 0, N, sigma)
         assert np.abs(got[b] - ref).max() < 2e-6, b
+
+
+def test_grf_large_image_covariance(torch_cuda):
+    """Large periods (the filter spectrum's rounding-level negatives are zeros)."""
+    torch = torch_cuda
+    N, ell = 4096, 8.0
+    raw = torch.zeros((1, N, N), device="cuda")
+    srk.grf(raw, ell, 5, minmax=False)
+    torch.cuda.synchronize()
+    r = host(raw)[0]
+    r = (r - r.mean()) / r.std()
+    for d in (8, 16):
+        emp = np.mean(r[d:, :] * r[:-d, :])
+        assert abs(emp - np.exp(-d * d / (2 * ell * ell))) < 0.03, d
