@@ -39,6 +39,9 @@ inline srk_status fail(srk_status s, const char* fmt, ...) {
 
 inline srk_status cuda_status(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return SRK_OK;
+  // a failed allocation is not sticky: clear it so the next launch check
+  // does not report it again
+  if (e == cudaErrorMemoryAllocation) (void)cudaGetLastError();
   return fail(e == cudaErrorMemoryAllocation ? SRK_ERR_ALLOC : SRK_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 

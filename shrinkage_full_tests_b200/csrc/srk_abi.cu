@@ -14,12 +14,23 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "internal.h"
 #include "spectra.cuh"
 
 using namespace srk;
 
 namespace {
+
+// One NVTX range per operator call (visible in Nsight timelines; a no-op
+// without a tool attached).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Host double-precision twiddle table (cos, sin)(2 pi m / M).
 std::vector<double2> twiddles64(int M) {
@@ -548,6 +559,7 @@ namespace {
 
 srk_status op_training_forward(const void* E, const void* I, const void* gx, const void* gy, int N, int W,
                                int erosion, float dx, int B, srk_stream_t s, void* R, srk_plan p) {
+  const NvtxRange nvtx_range("srk_training_forward");
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(E);
@@ -564,6 +576,7 @@ srk_status op_training_forward(const void* E, const void* I, const void* gx, con
 
 srk_status op_forward_oas(const void* E, const void* I, const void* gx, const void* gy, int N, int W, int erosion,
                           float dx, srk_stream_t s, void* R, srk_plan p, void* ux, void* uy) {
+  const NvtxRange nvtx_range("srk_forward_oas");
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(E);
   SRK_NONNULL(I);
@@ -577,6 +590,7 @@ srk_status op_forward_oas(const void* E, const void* I, const void* gx, const vo
 
 srk_status op_adjoint(const void* v, const void* ux, const void* uy, const void* I, const void* gx, const void* gy,
                       int N, int W, int erosion, float dx, srk_stream_t s, void* dLdI, void* dLdE, srk_plan p) {
+  const NvtxRange nvtx_range("srk_adjoint");
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(v);
   SRK_NONNULL(ux);
@@ -592,6 +606,7 @@ srk_status op_adjoint(const void* v, const void* ux, const void* uy, const void*
 
 srk_status op_tangent(const void* f, const void* g, const void* df, const void* dg, const void* gx, const void* gy,
                       int N, int W, int erosion, float dx, srk_stream_t s, void* dh, srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent");
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);
@@ -608,6 +623,7 @@ srk_status op_tangent(const void* f, const void* g, const void* df, const void* 
 srk_status op_tangent_adjoint(const void* f, const void* g, const void* df, const void* dg, const void* lam,
                               const void* dlam, const void* gx, const void* gy, int N, int W, int erosion, float dx,
                               srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent_adjoint");
   SRK_TRY(check_dims(p, N, W, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);
@@ -629,6 +645,7 @@ srk_status op_tangent_adjoint(const void* f, const void* g, const void* df, cons
 }
 
 srk_status op_forward(const void* f, const void* g, int B, srk_stream_t s, void* h, srk_plan p) {
+  const NvtxRange nvtx_range("srk_forward");
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(f);
@@ -643,6 +660,7 @@ srk_status op_forward(const void* f, const void* g, int B, srk_stream_t s, void*
 
 srk_status op_vjp(const void* v, const void* f, const void* g, int B, srk_stream_t s, void* dLdf, void* dLdg,
                   srk_plan p) {
+  const NvtxRange nvtx_range("srk_vjp");
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(v);
@@ -664,6 +682,7 @@ srk_status op_vjp(const void* v, const void* f, const void* g, int B, srk_stream
 
 srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, int B, srk_stream_t s, void* dh,
                   srk_plan p) {
+  const NvtxRange nvtx_range("srk_jvp");
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(check_batch(p, B));
   SRK_NONNULL(f);
@@ -784,6 +803,7 @@ srk_status check_ragged(const srk_plan_s* p, int erosion, float dx) {
 
 srk_status op_forward_oas_ragged(const void* E, const void* I, const void* gx, const void* gy, int B, const int* Ns,
                                  int erosion, float dx, srk_stream_t s, void* R, srk_plan p) {
+  const NvtxRange nvtx_range("srk_forward_oas_ragged");
   SRK_TRY(check_ragged(p, erosion, dx));
   SRK_NONNULL(E);
   SRK_NONNULL(I);
@@ -799,6 +819,7 @@ srk_status op_forward_oas_ragged(const void* E, const void* I, const void* gx, c
 srk_status op_adjoint_ragged(const void* v, const void* ux, const void* uy, const void* I, const void* gx,
                              const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s, void* dLdI,
                              void* dLdE, srk_plan p) {
+  const NvtxRange nvtx_range("srk_adjoint_ragged");
   SRK_TRY(check_ragged(p, erosion, dx));
   SRK_NONNULL(v);
   SRK_NONNULL(ux);
@@ -818,6 +839,7 @@ srk_status op_adjoint_ragged(const void* v, const void* ux, const void* uy, cons
 srk_status op_tangent_ragged(const void* f, const void* g, const void* df, const void* dg, const void* gx,
                              const void* gy, int B, const int* Ns, int erosion, float dx, srk_stream_t s, void* dh,
                              srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent_ragged");
   SRK_TRY(check_ragged(p, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);
@@ -835,6 +857,7 @@ srk_status op_tangent_ragged(const void* f, const void* g, const void* df, const
 srk_status op_tangent_adjoint_ragged(const void* f, const void* g, const void* df, const void* dg, const void* lam,
                                      const void* dlam, const void* gx, const void* gy, int B, const int* Ns,
                                      int erosion, float dx, srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent_adjoint_ragged");
   SRK_TRY(check_ragged(p, erosion, dx));
   SRK_NONNULL(f);
   SRK_NONNULL(g);

@@ -272,6 +272,24 @@ def test_bounded_wait_gives_up_and_context_survives(torch_cuda):
     assert rel_max_err(host(R)[0], O.forward(host(E)[0], host(E)[0], Kx, Ky, 15, 1.0)) < 1e-3
 
 
+def test_failed_allocation_reports_alloc_and_context_survives(torch_cuda):
+    """A plan whose scratch cannot be allocated (65535 work tiles of a 512
+    tile, ~350 GB) fails with SRK_ERR_ALLOC; nothing is left half-built and
+    the device keeps working."""
+    torch = torch_cuda
+    with pytest.raises(srk.SrkError) as ei:
+        srk.SrkPlan(512, 392, 60, 1.0, 1_000_000, tile_M=512, scratch_budget=1 << 40)
+    assert ei.value.status == srk.SRK_ERR_ALLOC
+    plan = srk.SrkPlan(128, 98, 15, 1.0, 2)
+    Kx, Ky = kernel(31)
+    GX, GY = spectra(Kx, Ky, 128, torch)
+    E = dev(np.stack(fields(128, 2, 6)), torch)
+    R = torch.zeros((2, 98, 98), device="cuda")
+    srk.srkTrainingForward(E, E, GX, GY, 128, 98, 15, 1.0, 2, None, R, plan)
+    plan.sync()
+    assert rel_max_err(host(R)[1], O.forward(host(E)[1], host(E)[1], Kx, Ky, 15, 1.0)) < 1e-3
+
+
 @pytest.mark.parametrize("dtype", ["f16", "bf16"])
 @pytest.mark.parametrize("N,KW,B", [(256, 31, 3), (512, 121, 2)])
 def test_half_storage_training_forward(torch_cuda, dtype, N, KW, B):
