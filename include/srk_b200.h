@@ -51,12 +51,13 @@ typedef enum srk_dtype { SRK_F32 = 0, SRK_F16 = 1, SRK_BF16 = 2 } srk_dtype;
  * for even kernels and differ by a sign for the odd Green's tensor. */
 typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_adj_convention;
 
-/* Kernel schedule of the convolution engine.  PERSISTENT (default): one
- * launch per call; the column/row/column passes of every work tile run as
- * tickets of a queue with their intermediates in an L2-resident ring.
- * THREE_PASS: three launches per chunk of work tiles with the intermediates
- * in a device scratch buffer (used for A/B measurement and as the fallback
- * when the scratch budget holds fewer than three work tiles). */
+/* Kernel schedule of the convolution engine.  THREE_PASS (default): three
+ * launches per chunk of work tiles with the intermediates in a device
+ * scratch buffer.  PERSISTENT: one launch per call; the column/row/column
+ * passes of every work tile run as tickets of a queue with their
+ * intermediates in an L2-resident ring (falls back to THREE_PASS when the
+ * scratch holds fewer than three work tiles).  SRK_TILE_AUTOTUNE plans time
+ * both and keep the faster. */
 typedef enum srk_schedule { SRK_SCHEDULE_PERSISTENT = 0, SRK_SCHEDULE_THREE_PASS = 1 } srk_schedule;
 
 typedef struct srk_plan_info {
