@@ -17,7 +17,7 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   constexpr int K = OpTraits<OP>::K;
   constexpr int L = OpTraits<OP>::L;
   const size_t sm1 = phase_smem_bytes<M>();
-  const size_t sm2 = sm1;
+  const size_t sm2 = sm1 + p2_tile_bytes<M>(g.S);
   const size_t sm3 = sm1 + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
   const size_t per = wt_elems<M, OP>(g.S);
   const size_t cap = p->scratch_bytes / sizeof(float2) / per;  // WTs that fit the scratch

@@ -606,10 +606,29 @@ __host__ __device__ constexpr int row_stride() {
   while (w % 8 != (lpu_of<M>() == 4 ? 4 : 2)) ++w;
   return w;
 }
-// S2 rows are padded to a multiple of 8 columns (16-byte aligned float4 reads).
+// Valid columns x' of S2 rounded up to a multiple of 8 (>= LPU).
 __host__ __device__ inline int s2_pitch(int S) { return (S + 7) & ~7; }
+// S2 layout.  Blocked (M = 512, LPU = 4): S2[l][x'/LPU][ky][x' % LPU], so
+// the LPU columns a P3 unit needs are one contiguous run of M*LPU values
+// (instead of 32-byte pieces of every row), and the LPU x LPU block a P2
+// unit produces per column block is contiguous too; P2 assembles the blocks
+// in a shared tile of pitch s2_block_pitch per block (LPU^2 values + padding
+// that keeps its writes free of bank conflicts).  Row layout (LPU = 8):
+// S2[l][ky][x'], pitch s2_pitch(S) — with 64-byte pieces per row the extra
+// tile pass in P2 costs more than it saves in P3.
+template <int M>
+__host__ __device__ constexpr bool s2_blocked() { return lpu_of<M>() == 4; }
+template <int M>
+__host__ __device__ constexpr int s2_block_pitch() { return lpu_of<M>() == 4 ? 20 : 72; }
+template <int M>
+__host__ __device__ inline size_t p2_tile_bytes(int S) {
+  return s2_blocked<M>() ? sizeof(float2) * (size_t)(s2_pitch(S) / lpu_of<M>()) * s2_block_pitch<M>() : 0;
+}
+// Twiddle slots at the start of every kernel's shared memory.
+template <int M>
+__host__ __device__ constexpr int tw_slots() { return (tw_entries(M) + 7) & ~7; }
 
-// Scratch of one work tile: S1 [K][x < M][ky < M] then S2 [L][ky < M][x' < pitch(S)] (float2).
+// Scratch of one work tile: S1 [K][x < M][ky < M] then S2 (L fields of M x pitch(S), see above) (float2).
 template <int M, int OP>
 __host__ __device__ constexpr size_t s1_elems() { return (size_t)OpTraits<OP>::K * M * M; }
 template <int M, int OP>
@@ -617,9 +636,10 @@ __host__ __device__ inline size_t wt_elems(int S) {
   return s1_elems<M, OP>() + (size_t)OpTraits<OP>::L * M * s2_pitch(S);
 }
 
-// Shared memory of every phase: the twiddle table and 2 x LPU staging rows.
+// Shared memory of every phase: the twiddle table and 2 x LPU staging rows
+// (P2 adds its block tile, P3 its first gradient window).
 template <int M>
-constexpr size_t phase_smem_bytes() { return sizeof(float2) * (M + 2 * lpu_of<M>() * row_stride<M>()); }
+constexpr size_t phase_smem_bytes() { return sizeof(float2) * (tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()); }
 
 // Copies between a thread's registers (strided order) and a padded row.
 template <int M>
@@ -688,7 +708,7 @@ template <int M, int OP>
 __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __restrict__ S2,
                                        const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG,
                                        const Geom& g, int ky0, float2* __restrict__ rows,
-                                       const float2* __restrict__ tw, int line, int t) {
+                                       const float2* __restrict__ tw, int line, int t, float2* __restrict__ tile) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int RSP = TPF + TPF / 16;
@@ -707,13 +727,34 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
   const float2* gxr = Gx + (size_t)ky * M + t;
   const float2* gyr = Gy + (size_t)ky * M + t;
   auto spec = [&](float2 z, float2 G) { return conjG ? cmulc(z, G) : cmul(z, G); };
+  // valid columns of field l -> the shared block tile -> whole LPU x LPU
+  // blocks of S2 (16-byte stores, each block one contiguous run)
+  constexpr int PB = s2_block_pitch<M>();
+  constexpr int F4B = LPU * LPU / 2;  // float4 per block
+  const int nblk = P / LPU;
   auto emit = [&](const float2 (&o)[EPT], int l) {
-    float2* dst = S2 + ((size_t)l * M + ky) * P - e + t;
+    if constexpr (!s2_blocked<M>()) {
+      float2* dst = S2 + ((size_t)l * M + ky) * P - e + t;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) {
+        const int xv = t + TPF * i - e;
+        if (xv >= 0 && xv < S) __stcg(dst + TPF * i, o[i]);
+      }
+      return;
+    }
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       const int xv = t + TPF * i - e;
-      if (xv >= 0 && xv < S) __stcg(dst + TPF * i, o[i]);
+      if (xv >= 0 && xv < S) tile[(xv / LPU) * PB + line * LPU + (xv % LPU)] = o[i];
     }
+    __syncthreads();
+    float2* dst = S2 + ((size_t)l * nblk * M + ky0) * LPU;
+    for (int j = threadIdx.x; j < nblk * F4B; j += kThreads) {
+      const int q = j / F4B, w = j - (j / F4B) * F4B;
+      const float4 v = *reinterpret_cast<const float4*>(tile + q * PB + 2 * w);
+      __stcg(reinterpret_cast<float4*>(dst + (size_t)q * M * LPU + 2 * w), v);
+    }
+    __syncthreads();  // the tile is reused by the next field
   };
   float2 z[EPT];
   row_to_regs<M>(row0, z, t);
@@ -795,7 +836,12 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
     if (a.e >= 1) issue_window(0, win0);  // in flight during the staging and the transforms
   }
 #pragma unroll
-  for (int l = 0; l < L; ++l) stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
+  for (int l = 0; l < L; ++l) {
+    if constexpr (s2_blocked<M>())
+      stage_rows<M>(S2 + ((size_t)l * (P / LPU) + xb) * M * LPU, LPU, rows + l * LPU * RS);
+    else
+      stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
+  }
   __syncthreads();
   const int xv = x0 + line;
   const bool active = xv < g.S;
@@ -872,7 +918,7 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   load_twiddles(sm, twg, M);
   __syncthreads();
   const int wl = blockIdx.y;
-  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + M + line * row_stride<M>(),
+  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>() + line * row_stride<M>(),
                    sm, line, t);
 }
 
@@ -885,7 +931,9 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
   const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
   load_twiddles(sm, twg, M);
   float2* base = scratch + blockIdx.y * wt_elems<M, OP>(g.S);
-  phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, blockIdx.x * lpu_of<M>(), sm + M, sm, line, t);
+  float2* rows = sm + tw_slots<M>();
+  phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, blockIdx.x * lpu_of<M>(), rows, sm, line, t,
+                rows + 2 * lpu_of<M>() * row_stride<M>());
 }
 
 template <int M, int OP, typename T>
@@ -897,9 +945,9 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
   load_twiddles(sm, twg, M);
   const int wl = blockIdx.y;
   constexpr bool ASYNC = p3_async_window<OP, T>();
-  float* win0 = ASYNC ? reinterpret_cast<float*>(sm + M + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
+  float* win0 = ASYNC ? reinterpret_cast<float*>(sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
   phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
-                          sm + M, sm, line, t, win0);
+                          sm + tw_slots<M>(), sm, line, t, win0);
 }
 
 // ---- persistent schedule ---------------------------------------------------------
@@ -977,7 +1025,7 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
   const size_t slot_elems = wt_elems<M, OP>(g.S);
   unsigned long long spins = 0;
   float2* tw = sm;
-  float2* buf = sm + M;
+  float2* buf = sm + tw_slots<M>();
   load_twiddles(tw, twg, M);
   if (threadIdx.x == 0) s_t[0] = (int)atomicAdd(&ctl->ticket, 1u);
   __syncthreads();
@@ -1010,7 +1058,8 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
       if (phase == 1) {
         phase1<M, OP, T>(a, g, w, unit, base, buf + line * row_stride<M>(), tw, line, t);
       } else if (phase == 2) {
-        phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * LPU, buf, tw, line, t);
+        phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * LPU, buf, tw, line, t,
+                      buf + 2 * LPU * row_stride<M>());
       } else {
         phase3<M, OP, T>(base + s1_elems<M, OP>(), a, g, w, unit, buf, tw, line, t);
       }
