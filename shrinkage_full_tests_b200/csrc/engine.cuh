@@ -618,6 +618,10 @@ __host__ __device__ inline int s2_pitch(int S) { return (S + 7) & ~7; }
 // tile pass in P2 costs more than it saves in P3.
 template <int M>
 __host__ __device__ constexpr bool s2_blocked() { return lpu_of<M>() == 4; }
+// S1 likewise (M = 512): S1[k][ky/LPU][x][ky % LPU], assembled by P1 in its
+// staging rows, staged by P2 from one contiguous run of M*LPU values.
+template <int M>
+__host__ __device__ constexpr bool s1_blocked() { return lpu_of<M>() == 4; }
 template <int M>
 __host__ __device__ constexpr int s2_block_pitch() { return lpu_of<M>() == 4 ? 20 : 72; }
 template <int M>
@@ -660,19 +664,43 @@ __device__ __forceinline__ void regs_to_row(float2* __restrict__ row, const floa
 // P1: line `line` transforms column x = xb*LPU + line of every field along y.
 template <int M, int OP, typename T>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
-                                       float2* __restrict__ row, const float2* __restrict__ tw, int line, int t) {
+                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int K = OpTraits<OP>::K;
-  const int x = xb * lpu_of<M>() + line;
+  constexpr int LPU = lpu_of<M>();
+  constexpr int RS = row_stride<M>();
+  const int x = xb * LPU + line;
+  float2* row = rows + line * RS;
 #pragma unroll 1
   for (int k = 0; k < K; ++k) {
     float2 z[EPT];
     load_column<M, OP, T>(a, g, w, k, x, t, z);
     fft<M, false>(z, row, tw, t, 1 + line);
-    float2* dst = S1 + ((size_t)k * M + x) * M + t;
+    if constexpr (s1_blocked<M>()) {
+      // the unit's LPU columns -> shared tile of (ky/LPU) blocks -> whole
+      // LPU x LPU blocks of S1 (the staging rows are free after the transforms)
+      constexpr int PB = s2_block_pitch<M>();
+      constexpr int F4B = LPU * LPU / 2;
+      __syncthreads();
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) __stcg(dst + TPF * i, z[i]);
+      for (int i = 0; i < EPT; ++i) {
+        const int ky = t + TPF * i;
+        rows[(ky / LPU) * PB + line * LPU + (ky % LPU)] = z[i];
+      }
+      __syncthreads();
+      float2* dst = S1 + (size_t)k * M * M + (size_t)xb * LPU * LPU;
+      for (int j = threadIdx.x; j < (M / LPU) * F4B; j += kThreads) {
+        const int q = j / F4B, v = j - (j / F4B) * F4B;
+        __stcg(reinterpret_cast<float4*>(dst + (size_t)q * M * LPU + 2 * v),
+               *reinterpret_cast<const float4*>(rows + q * PB + 2 * v));
+      }
+      __syncthreads();  // the rows are the next field's exchange rows
+    } else {
+      float2* dst = S1 + ((size_t)k * M + x) * M + t;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) __stcg(dst + TPF * i, z[i]);
+    }
   }
 }
 
@@ -719,7 +747,12 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
   const int bar = 1 + line;
   // S1[k][x][ky0 + c]: a transposing copy of LPU consecutive ky of every column x
 #pragma unroll
-  for (int k = 0; k < K; ++k) stage_rows<M>(S1 + (size_t)k * M * M + ky0, M, rows + k * LPU * RS);
+  for (int k = 0; k < K; ++k) {
+    if constexpr (s1_blocked<M>())
+      stage_rows<M>(S1 + (size_t)k * M * M + (size_t)ky0 * M, LPU, rows + k * LPU * RS);
+    else
+      stage_rows<M>(S1 + (size_t)k * M * M + ky0, M, rows + k * LPU * RS);
+  }
   __syncthreads();
   const int ky = ky0 + line;
   float2* row0 = rows + line * RS;           // field 0 / exchange
@@ -918,7 +951,7 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   load_twiddles(sm, twg, M);
   __syncthreads();
   const int wl = blockIdx.y;
-  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>() + line * row_stride<M>(),
+  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(),
                    sm, line, t);
 }
 
@@ -1056,7 +1089,7 @@ k_persist(OpArgs a, Geom g, const float2* __restrict__ Gx, const float2* __restr
     if (live) {
       float2* base = scratch + (size_t)slot * slot_elems;
       if (phase == 1) {
-        phase1<M, OP, T>(a, g, w, unit, base, buf + line * row_stride<M>(), tw, line, t);
+        phase1<M, OP, T>(a, g, w, unit, base, buf, tw, line, t);
       } else if (phase == 2) {
         phase2<M, OP>(base, base + s1_elems<M, OP>(), Gx, Gy, conjG, g, unit * LPU, buf, tw, line, t,
                       buf + 2 * LPU * row_stride<M>());
