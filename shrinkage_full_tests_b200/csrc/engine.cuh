@@ -619,7 +619,9 @@ __host__ __device__ inline int s2_pitch(int S) { return (S + 7) & ~7; }
 template <int M>
 __host__ __device__ constexpr bool s2_blocked() { return lpu_of<M>() == 4; }
 // S1 likewise (M = 512): S1[k][ky/LPU][x][ky % LPU], assembled by P1 in its
-// staging rows, staged by P2 from one contiguous run of M*LPU values.
+// staging rows (free after the transforms), staged by P2 from one
+// contiguous run of M*LPU values.  At LPU = 8 the rows are read in 64-byte
+// pieces already and the blocked form measured no faster.
 template <int M>
 __host__ __device__ constexpr bool s1_blocked() { return lpu_of<M>() == 4; }
 template <int M>
