@@ -40,6 +40,15 @@
 #ifndef SRK_MIN_BLOCKS
 #define SRK_MIN_BLOCKS 4
 #endif
+#ifndef SRK_P1_MIN_BLOCKS
+#define SRK_P1_MIN_BLOCKS SRK_MIN_BLOCKS
+#endif
+#ifndef SRK_P2_MIN_BLOCKS
+#define SRK_P2_MIN_BLOCKS SRK_MIN_BLOCKS
+#endif
+#ifndef SRK_P3_MIN_BLOCKS
+#define SRK_P3_MIN_BLOCKS SRK_MIN_BLOCKS
+#endif
 
 namespace srk {
 
@@ -795,6 +804,19 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
   row_to_regs<M>(row0, z, t);
   fft<M, false>(z, row0, tw, t, bar);
   if constexpr (K == 1) {
+#ifdef SRK_P2_STASH_REGS
+    float2 zs[EPT];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) zs[i] = z[i];
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const float2* gr = l ? gyr : gxr;
+#pragma unroll
+      for (int i = 0; i < EPT; ++i) z[i] = spec(zs[i], __ldg(gr + TPF * i));
+      fft<M, true>(z, row0, tw, t, bar);
+      emit(z, l);
+    }
+#else
     regs_to_row<M>(row1, z, t);  // stash Z(ky, .): each thread rereads only its own elements
 #pragma unroll
     for (int l = 0; l < 2; ++l) {
@@ -805,6 +827,7 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
       fft<M, true>(z, row0, tw, t, bar);
       emit(z, l);
     }
+#endif
   } else {
     group_sync<TPF>(bar);
     regs_to_row<M>(row0, z, t);  // stash Z0(ky, .) in its own row
@@ -945,7 +968,7 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
 
 // ---- three-launch schedule (one kernel per phase over a chunk of WTs) ------
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SRK_P1_MIN_BLOCKS)
 k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
   extern __shared__ float2 sm[];
   constexpr int TPF = tpf_of<M>();
@@ -958,7 +981,7 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
 }
 
 template <int M, int OP>
-__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SRK_P2_MIN_BLOCKS)
 k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* __restrict__ Gy, int conjG, Geom g,
      const float2* __restrict__ twg) {
   extern __shared__ float2 sm[];
@@ -972,7 +995,7 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
 }
 
 template <int M, int OP, typename T>
-__global__ void __launch_bounds__(kThreads, SRK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kThreads, SRK_P3_MIN_BLOCKS)
 k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
   extern __shared__ float2 sm[];
   constexpr int TPF = tpf_of<M>();
