@@ -299,6 +299,9 @@ def run_ours(a):
     if not a.no_extra and world == 1:
         extra["fp16_storage"] = half_storage_rate(torch, srk, E, GX, GY, N, W, e, dx, B)
         extra["published_config"] = published_config_rate(torch, srk)
+        # the large single image of the configurations: N = 32768, KW = 121, GRF ell = 32 px
+        extra["large_image"] = ops_throughput(torch, srk, N=32768, KW=121, reps=1, spectra_M=2048, ell=32.0)
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -372,16 +375,16 @@ def published_config_rate(torch, srk, steps=20):
     return out
 
 
-def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
+def ops_throughput(torch, srk, N=4096, KW=61, reps=3, spectra_M=1024, ell=8.0):
     """Output Mpix/s of each OaS operator on one N x N image (one GPU)."""
     import numpy as np
     e = (KW - 1) // 2
     W = N - 2 * e
-    _, _, GX, GY = make_spectra(torch, srk, KW, 1024, 1.0)
-    f, g = grf_batch(torch, 2, N, 77)
+    _, _, GX, GY = make_spectra(torch, srk, KW, spectra_M, 1.0)
+    f, g = grf_batch(torch, 2, N, 77, ell=ell)
     df, dg = (1e-2 * torch.randn((2, N, N), device="cuda")).unbind(0)
     lam, dlam = torch.randn((2, W, W), device="cuda").unbind(0)
-    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=1024, tile_M=srk.SRK_TILE_AUTOTUNE)
+    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=spectra_M, tile_M=srk.SRK_TILE_AUTOTUNE)
     R = torch.empty((W, W), device="cuda")
     ux, uy = torch.empty_like(R), torch.empty_like(R)
     o1, o2 = torch.empty((N, N), device="cuda"), torch.empty((N, N), device="cuda")
@@ -392,7 +395,9 @@ def ops_throughput(torch, srk, N=4096, KW=61, reps=3):
         "tangent_adjoint": lambda: srk.shrinkageTangentAdjointOaS(f, g, df, dg, lam, dlam, GX, GY, N, W, e, 1.0,
                                                                    None, o1, o2, plan),
     }
-    out = {"config": "N=%d KW=%d B=1 fp32 tile_M=%d" % (N, KW, plan.info()["tile_M"])}
+    info = plan.info()
+    out = {"config": "N=%d KW=%d B=1 fp32 tile_M=%d spectra_M=%d" % (N, KW, info["tile_M"], spectra_M),
+           "library_workspace_bytes": info["scratch_bytes"] + 2 * W * W * 4 + 2 * info["tile_M"] ** 2 * 8}
     alg = {"forward": 2 * N * N + W * W, "adjoint": 3 * W * W + N * N + 2 * N * N,
            "tangent": 4 * N * N + W * W, "tangent_adjoint": 6 * N * N + 2 * W * W}
     peak, _ = measured_peaks()
@@ -442,7 +447,74 @@ def run_reference(a):
         "e2e": {"value": rate, "unit": "img/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     line["gpu_reference"] = gpu_reference(a)
+    line["gpu_reference_oas"] = gpu_reference_oas()
     print(json.dumps(line))
+
+
+def gpu_reference_oas(N=4096, KW=61, M=1024, reps=5):
+    """Reference-structure stand-in for srkForwardOaS (srk_forward.cuh:354-501),
+    whose cufftDX build is unavailable (MathDx is not installed): the same
+    per-tile loop — for each of Gx, Gy and each M x M tile (stride M - 2e):
+    2-D R2C FFT, product with the kernel spectrum, C2R, valid crop — then the
+    central differences and the combine, with cuFFT (through torch.fft) as
+    the tile FFT.  Timed on this GPU with CUDA events."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        import shrinkage_full_tests_b200 as srk
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        S = M - 2 * e
+        T = (W + S - 1) // S
+        Kx, Ky, _, _ = make_spectra(torch, srk, KW, M, 1.0)
+        # kernel spectra in the tile frame: kernel centred at the origin (the fftshift of the reference)
+        def spec(K):
+            P = torch.zeros((M, M), device="cuda")
+            P[:KW, :KW] = K
+            P = torch.roll(P, shifts=(-e, -e), dims=(0, 1))
+            return torch.fft.rfft2(P)
+        SX, SY = spec(Kx), spec(Ky)
+        f = grf_batch(torch, 1, N, 77)[0]
+        pad = torch.zeros((T * S + 2 * e, T * S + 2 * e), device="cuda")
+        pad[:N, :N] = f
+        ux = torch.empty((T * S, T * S), device="cuda")
+        uy = torch.empty_like(ux)
+
+        def step():
+            for G, u in ((SX, ux), (SY, uy)):
+                for tx in range(T):
+                    for ty in range(T):
+                        tile = pad[tx * S:tx * S + M, ty * S:ty * S + M]
+                        c = torch.fft.irfft2(torch.fft.rfft2(tile) * G, s=(M, M))
+                        u[tx * S:(tx + 1) * S, ty * S:(ty + 1) * S] = c[e:e + S, e:e + S]
+            fx = (f[e + 1:N - e + 1, e:N - e] - f[e - 1:N - e - 1, e:N - e]) * 0.5
+            fy = (f[e:N - e, e + 1:N - e + 1] - f[e:N - e, e - 1:N - e - 1]) * 0.5
+            return ux[:W, :W] * fx + uy[:W, :W] * fy
+
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            step()
+        s1.record()
+        torch.cuda.synchronize()
+        ms = s0.elapsed_time(s1) / reps
+        # the stand-in computes the same operator: compare with the library once
+        _, _, GXr, GYr = make_spectra(torch, srk, KW, M, 1.0)
+        plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=M)
+        R = torch.empty((W, W), device="cuda")
+        srk.srkForwardOaS(f, f, GXr, GYr, N, W, e, 1.0, None, R, plan)
+        torch.cuda.synchronize()
+        ref = step()
+        diff = float((R - ref).abs().max() / ref.abs().max())
+        return {"what": "reference-structure per-tile cuFFT stand-in for srkForwardOaS (cufftDX build unavailable)",
+                "config": "N=%d KW=%d M_TILE=%d, %d tiles per conv" % (N, KW, M, T * T), "ms": ms,
+                "out_mpix_per_s": W * W / (ms * 1e-3) / 1e6, "max_rel_diff_vs_library": diff}
+    except Exception as ex:  # noqa: BLE001
+        return {"unavailable": "%s" % ex}
 
 
 def gpu_reference(a):

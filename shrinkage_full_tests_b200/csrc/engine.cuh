@@ -447,6 +447,18 @@ __host__ __device__ constexpr int lpu_of() { return kThreads / tpf_of<M>(); }
 // gy0 - off (off = gy0 mod 4); otherwise off = 0.  The pitch is a multiple
 // of 4 floats (16-byte aligned columns).
 __host__ __device__ inline int gwin_pitch(int S) { return (S + 8) & ~3; }
+// The same for a window of raw storage values (16-byte chunks of EPC
+// elements): a multiple of EPC that holds off + S + 2 for any off < EPC.
+template <typename T>
+__host__ __device__ inline int gwin_pitch_t(int S) {
+  constexpr int EPC = 16 / (int)sizeof(T);
+  return (S + 2 + 2 * (EPC - 1)) / EPC * EPC;
+}
+// Shared-memory window value as float.
+template <typename T> __device__ __forceinline__ float swin(const T* p);
+template <> __device__ __forceinline__ float swin<float>(const float* p) { return *p; }
+template <> __device__ __forceinline__ float swin<__half>(const __half* p) { return __half2float(*p); }
+template <> __device__ __forceinline__ float swin<__nv_bfloat16>(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 // (LPU + 2) * gwin_pitch(S) floats <= (LPU + 2) * (M + 4) <= 2 * LPU * (M + M/16 + 2)
 // for S <= M - 2: one image's window always fits the LPU staging rows of the
 // second field.
@@ -488,26 +500,29 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// vec16: 16-byte chunks (needs N % 4 == 0 and a 16-byte aligned image, so
-// every chunk lies wholly inside or wholly outside the image); else 4-byte
-// copies.
-__device__ __forceinline__ void stage_grad_window_async(const float* __restrict__ img, int N, const GradWin& gw,
-                                                        bool vec16, float* __restrict__ dst) {
+// Raw storage values of the window.  vec16: 16-byte chunks of EPC values
+// (needs N % EPC == 0 and a 16-byte aligned image, so every chunk lies
+// wholly inside or wholly outside the image); else 4-byte copies (FP32 only).
+template <typename T>
+__device__ __forceinline__ void stage_grad_window_async(const T* __restrict__ img, int N, const GradWin& gw,
+                                                        bool vec16, T* __restrict__ dst) {
+  constexpr int EPC = 16 / (int)sizeof(T);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int c = warp; c < gw.ncol; c += kWarps) {
     const int gx = gw.gx0 + c;
     const bool colin = gx >= 0 && gx < N;
-    const float* col = img + (long long)(colin ? gx : 0) * N;
-    float* d = dst + c * gw.HP;
+    const T* col = img + (long long)(colin ? gx : 0) * N;
+    T* d = dst + c * gw.HP;
     if (vec16) {
       const int gya = gw.gy0 - gw.off;
-      const int nch = (gw.off + gw.S + 2 + 3) >> 2;
+      const int nch = (gw.off + gw.S + 2 + EPC - 1) / EPC;
       for (int q = lane; q < nch; q += 32) {
-        const int gy = gya + 4 * q;
+        const int gy = gya + EPC * q;
         const bool in = colin && gy >= 0 && gy < N;
-        cp_async16_zfill(d + 4 * q, in ? col + gy : img, in);
+        cp_async16_zfill(reinterpret_cast<float*>(d + EPC * q), reinterpret_cast<const float*>(in ? col + gy : img),
+                         in);
       }
-    } else {
+    } else if constexpr (std::is_same<T, float>::value) {
       for (int r = lane; r < gw.S + 2; r += 32) {
         const int gy = gw.gy0 + r;
         const bool in = colin && gy >= 0 && gy < N;
@@ -516,14 +531,15 @@ __device__ __forceinline__ void stage_grad_window_async(const float* __restrict_
     }
   }
 }
-// Floats of one staged window at tile size M (S <= M - 2 when erosion >= 1).
+// Floats of one staged window at tile size M (S <= M - 2 when erosion >= 1);
+// a window of 2-byte values needs at most (LPU + 2) * (M + 8) of them.
 template <int M>
 __host__ __device__ constexpr int p3_window_floats() { return (lpu_of<M>() + 2) * (M + 4); }
 // P3 of the three-launch schedule prefetches the first window asynchronously
-// into a buffer of its own (forward / tangent epilogues on FP32 images).
+// into a buffer of its own (forward / tangent epilogues).
 template <int OP, typename T>
 __host__ __device__ constexpr bool p3_async_window() {
-  return (OP == OP_FWD || OP == OP_JVP) && std::is_same<T, float>::value;
+  return OP == OP_FWD || OP == OP_JVP;
 }
 
 // Forward / tangent epilogue, round h, with the central differences read
@@ -532,19 +548,19 @@ __host__ __device__ constexpr bool p3_async_window() {
 // (window = f) leaves the f terms in z0.y, round 1 (window = df) adds the df
 // terms.  z0 stays stashed in the line's padded row (z0s = row + t +
 // (t >> 4), element i at z0s[(TPF + TPF/16) i]) to keep registers free.
-template <int M, int OP, typename T>
+template <int M, int OP, typename T, typename WT>
 __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, const TileRef& tr, int x, int line,
                                                 int t, int h, float2* __restrict__ z0s,
-                                                const float2 (&z1)[M / tpf_of<M>()], const float* __restrict__ win,
+                                                const float2 (&z1)[M / tpf_of<M>()], const WT* __restrict__ win,
                                                 const GradWin& gw) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int RSP = TPF + TPF / 16;
   const int W = tr.W;
-  const int rb = gw.off + t - g.e + 1;        // window row of element 0: y - e + 1, y = t
-  const float* cm = win + line * gw.HP + rb;  // image column gx - 1
-  const float* cc = cm + gw.HP;               // gx
-  const float* cp = cc + gw.HP;               // gx + 1
+  const int rb = gw.off + t - g.e + 1;     // window row of element 0: y - e + 1, y = t
+  const WT* cm = win + line * gw.HP + rb;  // image column gx - 1
+  const WT* cc = cm + gw.HP;               // gx
+  const WT* cp = cc + gw.HP;               // gx + 1
   const int ox = tr.x0 + x - g.e;
   if (!tr.live || ox >= tr.Wout) return;
   const unsigned vm = valid_rows<M>(g, tr, t);
@@ -561,8 +577,8 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
         const float2 z0i = z0s[RSP * i];
         const float ux = h ? z0i.y : z0i.x;
         const float uy = h ? z1[i].y : z1[i].x;
-        const float fx = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
-        const float fy = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+        const float fx = (swin(cp + TPF * i) - swin(cm + TPF * i)) * 0.5f;
+        const float fy = (swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1)) * 0.5f;
         stf(Rp, TPF * i, dot2(ux, fx, uy, fy));
       }
       return;
@@ -576,8 +592,8 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
       if (UX) stf(UX, ob + TPF * i, ux);
       if (UY) stf(UY, ob + TPF * i, uy);
       if (R) {
-        const float fx = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
-        const float fy = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+        const float fx = (swin(cp + TPF * i) - swin(cm + TPF * i)) * 0.5f;
+        const float fy = (swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1)) * 0.5f;
         stf(R, ob + TPF * i, dot2(ux, fx, uy, fy));
       }
     }
@@ -587,8 +603,8 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
       if (!(vm >> i & 1u)) continue;
-      const float dx_ = (cp[TPF * i] - cm[TPF * i]) * 0.5f;
-      const float dy_ = (cc[TPF * i + 1] - cc[TPF * i - 1]) * 0.5f;
+      const float dx_ = (swin(cp + TPF * i) - swin(cm + TPF * i)) * 0.5f;
+      const float dy_ = (swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1)) * 0.5f;
       float2 z0i = z0s[RSP * i];
       if (h == 0) {
         z0i.y = dot2(z0i.y, dx_, z1[i].y, dy_);
@@ -850,48 +866,54 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
 template <int M, int OP, typename T, bool ASYNC = false>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
-                                       float* __restrict__ win0 = nullptr) {
+                                       T* __restrict__ win0 = nullptr) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int L = OpTraits<OP>::L;
   constexpr int RS = row_stride<M>();
   constexpr int LPU = lpu_of<M>();
   constexpr bool GRAD = (OP == OP_FWD || OP == OP_JVP);
-  static_assert(!ASYNC || p3_async_window<OP, T>(), "asynchronous window only for FP32 forward / tangent");
+  static_assert(!ASYNC || p3_async_window<OP, T>(), "asynchronous window only for the forward / tangent");
+  constexpr int EPC = 16 / (int)sizeof(T);  // storage values per 16-byte copy
   const int P = s2_pitch(g.S);
   const int x0 = xb * LPU;
   const int bar = 1 + line;
   // window of round h: image (pair member h, or f / df) columns
   // x0+e-1 .. x0+e+LPU, rows y0+e-1 .. y0+e+S
-  auto window_of = [&](int h, const TileRef& tr, bool vec16) {
+  // raw: the asynchronous copy of storage values (else floats staged by the threads)
+  auto window_of = [&](int h, const TileRef& tr, bool vec16, bool raw) {
     GradWin gw;
     gw.gx0 = tr.x0 + x0 + a.e - 1;
     gw.gy0 = tr.y0 + a.e - 1;
     gw.ncol = LPU + 2;
     gw.S = g.S;
-    gw.HP = gwin_pitch(g.S);
-    gw.off = vec16 ? (gw.gy0 & 3) : 0;
+    gw.HP = raw ? gwin_pitch_t<T>(g.S) : gwin_pitch(g.S);
+    gw.off = vec16 ? (gw.gy0 % EPC) : 0;
     return gw;
   };
   auto tile_h = [&](int h) { return tile_of(g, OP == OP_FWD ? 2 * w + h : w); };
   auto image_h = [&](int h) { return static_cast<const T*>(OP == OP_FWD || h == 0 ? a.I : a.dI); };
-  // 16-byte window copies: N % 4 == 0, a 16-byte aligned image start
+  // 16-byte window copies: N % EPC == 0, a 16-byte aligned image start
   auto vec16_of = [&](int h, const TileRef& tr) {
-    return ASYNC && (tr.N & 3) == 0 &&
-           ((reinterpret_cast<uintptr_t>(image_h(h)) + sizeof(float) * (uintptr_t)tr.on) & 15) == 0;
+    return ASYNC && tr.N % EPC == 0 &&
+           ((reinterpret_cast<uintptr_t>(image_h(h)) + sizeof(T) * (uintptr_t)tr.on) & 15) == 0;
   };
-  auto issue_window = [&](int h, float* dst) {
+  auto issue_window = [&](int h, T* dst) {
     if constexpr (ASYNC) {
       const TileRef tr = tile_h(h);
       const bool vec16 = vec16_of(h, tr);
-      if (tr.live)
-        stage_grad_window_async(reinterpret_cast<const float*>(image_h(h)) + tr.on, tr.N, window_of(h, tr, vec16),
-                                vec16, dst);
+      if (tr.live) stage_grad_window_async<T>(image_h(h) + tr.on, tr.N, window_of(h, tr, vec16, true), vec16, dst);
       cp_async_commit();
     }
   };
+  // 2-byte storage needs the 16-byte form for both windows; else the
+  // threads stage converted floats (below)
+  bool async_win = false;
   if constexpr (ASYNC) {
-    if (a.e >= 1) issue_window(0, win0);  // in flight during the staging and the transforms
+    async_win = a.e >= 1;
+    if constexpr (!std::is_same<T, float>::value)
+      async_win = async_win && vec16_of(0, tile_h(0)) && vec16_of(1, tile_h(1));
+    if (async_win) issue_window(0, win0);  // in flight during the staging and the transforms
   }
 #pragma unroll
   for (int l = 0; l < L; ++l) {
@@ -921,10 +943,10 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
     for (int i = 0; i < EPT; ++i) z1[i] = make_float2(0.f, 0.f);
   }
   if constexpr (ASYNC) {
-    if (a.e >= 1) {
+    if (async_win) {
       // window 0 has been arriving in its own buffer; window 1 goes to the
       // second field's rows once every line is done with them
-      float* win1 = reinterpret_cast<float*>(rows + LPU * RS);
+      T* win1 = reinterpret_cast<T*>(rows + LPU * RS);
       float2* z0s = row0 + t + (t >> 4);
       __syncthreads();
       issue_window(1, win1);
@@ -932,12 +954,14 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
       __syncthreads();
       const TileRef tr0 = tile_h(0);
       if (active)
-        epilogue_staged<M, OP, T>(a, g, tr0, xv + g.e, line, t, 0, z0s, z1, win0, window_of(0, tr0, vec16_of(0, tr0)));
+        epilogue_staged<M, OP, T, T>(a, g, tr0, xv + g.e, line, t, 0, z0s, z1, win0,
+                                     window_of(0, tr0, vec16_of(0, tr0), true));
       cp_async_wait<0>();
       __syncthreads();
       const TileRef tr1 = tile_h(1);
       if (active)
-        epilogue_staged<M, OP, T>(a, g, tr1, xv + g.e, line, t, 1, z0s, z1, win1, window_of(1, tr1, vec16_of(1, tr1)));
+        epilogue_staged<M, OP, T, T>(a, g, tr1, xv + g.e, line, t, 1, z0s, z1, win1,
+                                     window_of(1, tr1, vec16_of(1, tr1), true));
       return;
     }
   }
@@ -950,10 +974,10 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
       for (int h = 0; h < 2; ++h) {
         __syncthreads();  // rows of field 1 no longer used (round 0) / window consumed (round 1)
         const TileRef tr = tile_h(h);
-        const GradWin gw = window_of(h, tr, false);
+        const GradWin gw = window_of(h, tr, false, false);
         if (tr.live) stage_grad_window<T>(image_h(h) + tr.on, tr.N, gw, win);
         __syncthreads();
-        if (active) epilogue_staged<M, OP, T>(a, g, tr, xv + g.e, line, t, h, z0s, z1, win, gw);
+        if (active) epilogue_staged<M, OP, T, float>(a, g, tr, xv + g.e, line, t, h, z0s, z1, win, gw);
       }
       return;
     }
@@ -1003,7 +1027,7 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
   load_twiddles(sm, twg, M);
   const int wl = blockIdx.y;
   constexpr bool ASYNC = p3_async_window<OP, T>();
-  float* win0 = ASYNC ? reinterpret_cast<float*>(sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
+  T* win0 = ASYNC ? reinterpret_cast<T*>(sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
   phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
                           sm + tw_slots<M>(), sm, line, t, win0);
 }
