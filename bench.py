@@ -448,6 +448,7 @@ def run_reference(a):
     }
     line["gpu_reference"] = gpu_reference(a)
     line["gpu_reference_oas"] = gpu_reference_oas()
+    line["gpu_reference_cudnn"] = gpu_reference_cudnn(a)
     print(json.dumps(line))
 
 
@@ -513,6 +514,53 @@ def gpu_reference_oas(N=4096, KW=61, M=1024, reps=5):
         return {"what": "reference-structure per-tile cuFFT stand-in for srkForwardOaS (cufftDX build unavailable)",
                 "config": "N=%d KW=%d M_TILE=%d, %d tiles per conv" % (N, KW, M, T * T), "ms": ms,
                 "out_mpix_per_s": W * W / (ms * 1e-3) / 1e6, "max_rel_diff_vs_library": diff}
+    except Exception as ex:  # noqa: BLE001
+        return {"unavailable": "%s" % ex}
+
+
+def gpu_reference_cudnn(a, B=20, reps=2):
+    """The reference's cuDNN forward (training/srk_cudnn_forward.cuh:194-269,
+    built from its sources) on a bounded batch of the same workload, scaled
+    to images/s; None if unavailable."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from tests.gpu_util import ref_gpu
+        L = ref_gpu()
+        if L is None:
+            return {"unavailable": "oracle/_ref/libref_gpu.so not built"}
+        import shrinkage_full_tests_b200 as srk
+        N, KW, dx = a.N, a.KW, a.dx
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        Kx, Ky, GX, GY = make_spectra(torch, srk, KW, N, dx)
+        E = grf_batch(torch, B, N, 17)
+        R = torch.empty((B, W, W), device="cuda")
+        st = torch.cuda.current_stream().cuda_stream
+        ws = L.ref_cudnn_ws_create(N, W, KW, B, st)
+        call = lambda: L.ref_cudnn_forward(E.data_ptr(), E.data_ptr(), Kx.data_ptr(), Ky.data_ptr(), N, W, e, dx, B,
+                                           st, R.data_ptr(), ws)
+        assert call() == 0
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            call()
+        s1.record()
+        torch.cuda.synchronize()
+        ms = s0.elapsed_time(s1) / reps
+        L.ref_cudnn_ws_destroy(ws, st)
+        plan = srk.SrkPlan(N, W, e, dx, B)
+        Rl = torch.empty_like(R)
+        srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, Rl, plan)
+        torch.cuda.synchronize()
+        diff = float((Rl - R).abs().max() / R.abs().max())
+        return {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "B": B,
+                "what": "reference srkCudnnForward (cuDNN heuristic algorithm) compiled for sm_100a from its sources, "
+                        "bounded batch of the same workload",
+                "max_rel_diff_vs_library": diff}
     except Exception as ex:  # noqa: BLE001
         return {"unavailable": "%s" % ex}
 

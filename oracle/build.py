@@ -62,7 +62,7 @@ def build_reference(force=False):
     if force or _stale(gpu_out, gpu_src):
         _run([NVCC, "-std=c++17", "-O2", "--extended-lambda"] + ARCH +
              ["-Xcompiler", "-fPIC", "-shared", "-I" + inc, "-I" + os.path.join(REF_SRC, "training")] +
-             gpu_src + ["-lcufft", "-o", gpu_out])
+             gpu_src + ["-lcufft", "-lcudnn", "-o", gpu_out])
     return REF_OUT
 
 

@@ -4,7 +4,9 @@
 // the reference unmodified on the same device:
 //   srkTrainingForward + SrkTrainWorkspace   training/srk_training_forward.cuh:117-241
 //   MeasureCD_Batched                        third_party/src/metricUtil/cd_measure_util.cu:310-437
+//   srkCudnnForward + SrkCudnnWorkspace      training/srk_cudnn_forward.cuh:92-269
 #include "srk_training_forward.cuh"
+#include "srk_cudnn_forward.cuh"
 #include <metricUtil/cd_measure_util.cuh>
 #include <cstring>
 
@@ -37,3 +39,23 @@ extern "C" int ref_measure_cd(const float* d_sig, int B, int n, int L, int A, cu
   }
   return (int)cudaGetLastError();
 }
+
+// The reference's cuDNN forward (spatial kernels, column-major KW x KW).
+extern "C" void* ref_cudnn_ws_create(int N, int W, int KW, int B, cudaStream_t s) {
+  auto* w = new SrkCudnnWorkspace();
+  w->allocate(B, N, KW, KW, W, s);
+  cudaStreamSynchronize(s);
+  return w;
+}
+extern "C" void ref_cudnn_ws_destroy(void* w, cudaStream_t s) {
+  auto* ws = static_cast<SrkCudnnWorkspace*>(w);
+  ws->release(s);
+  cudaStreamSynchronize(s);
+  delete ws;
+}
+extern "C" int ref_cudnn_forward(const float* E, const float* I, const float* Kx, const float* Ky, int N, int W,
+                                 int erosion, float dx, int B, cudaStream_t s, float* R, void* w) {
+  srkCudnnForward(E, I, Kx, Ky, N, W, erosion, dx, B, s, R, *static_cast<SrkCudnnWorkspace*>(w));
+  return (int)cudaGetLastError();
+}
+

@@ -25,8 +25,8 @@ def spectra(Kx, Ky, M, torch):
 
 
 def ref_gpu():
-    """The reference's own srkTrainingForward / MeasureCD_Batched built from
-    its sources (oracle/_ref), or None."""
+    """The reference's own srkTrainingForward / srkCudnnForward /
+    MeasureCD_Batched built from its sources (oracle/_ref), or None."""
     global _ref_gpu
     if _ref_gpu is None:
         path = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
@@ -42,5 +42,10 @@ def ref_gpu():
         fp = ctypes.POINTER(ctypes.c_float)
         L.ref_measure_cd.argtypes = [P, I, I, I, I, P, fp, fp, fp]
         L.ref_measure_cd.restype = I
+        L.ref_cudnn_ws_create.argtypes = [I, I, I, I, P]
+        L.ref_cudnn_ws_create.restype = P
+        L.ref_cudnn_ws_destroy.argtypes = [P, P]
+        L.ref_cudnn_forward.argtypes = [P, P, P, P, I, I, I, F, I, P, P, P]
+        L.ref_cudnn_forward.restype = I
         _ref_gpu = L
     return _ref_gpu
