@@ -245,6 +245,14 @@ srk_status srk_measure_cd(const float* d_sig, int B, int n, int L, int A, srk_st
 srk_status srk_cd_after_shrinkage(const float* d_E, const float* d_R, int B, int N, int W, int erosion, float coeff,
                                   int axis, int L, int A, srk_stream_t stream, float* d_left, float* d_right,
                                   float* d_cd);
+/* The same CD without the full operator: R is computed on the measured line
+ * only, by direct convolution with the spatial kernels d_Kx, d_Ky
+ * (column-major KW x KW, KW odd <= min(2*erosion+1, 129)) — the strip idea of
+ * training/main_compare.cu:70-133.  Signal E + coeff*R with R from E and I
+ * (the training forward has E = I); erosion >= 1. */
+srk_status srk_cd_strip(const float* d_E, const float* d_I, const float* d_Kx, const float* d_Ky, int KW, int N,
+                        int W, int erosion, float dx, int B, float coeff, int axis, int L, int A, srk_stream_t stream,
+                        float* d_left, float* d_right, float* d_cd);
 
 /* ---- training forward without any device allocation ---------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -86,6 +86,7 @@ _SIGS = {
     "srk_forward": [_P, _P, _I, _P, _P, _P],
     "srk_vjp": [_P, _P, _P, _I, _P, _P, _P, _P],
     "srk_jvp": [_P, _P, _P, _P, _I, _P, _P, _P],
+    "srk_cd_strip": [_P, _P, _P, _P, _I, _I, _I, _I, _F, _I, _F, _I, _I, _I, _P, _P, _P, _P],
     "srk_grf": [_I, _I, _D, ctypes.c_ulonglong, _I, _P, _P],
     "srk_grf_filter": [_P, _I, _I, _D, _I, _P, _P],
     "srk_lns": [_I, _I, _P, _F, _F, _I, _P, _P],
@@ -337,4 +338,15 @@ def cd_after_shrinkage(E, R, N, W, erosion, coeff, axis, L=16, A=8, stream=None)
     out = [torch.empty(B, device=E.device, dtype=torch.float32) for _ in range(3)]
     _check(lib().srk_cd_after_shrinkage(_ptr(E), _ptr(R), B, N, W, erosion, coeff, axis, L, A, _stream(stream),
                                         *[_ptr(t) for t in out]))
+    return tuple(out)
+
+
+def cd_strip(E, I, Kx, Ky, N, W, erosion, dx, coeff, axis, L=16, A=8, stream=None):
+    """CD of the centre row (axis 0) or column (axis 1) of E_crop + coeff*R,
+    with R computed on that line only (spatial kernels Kx, Ky, KW x KW)."""
+    import torch
+    B = E.shape[0]
+    out = [torch.empty(B, device=E.device, dtype=torch.float32) for _ in range(3)]
+    _check(lib().srk_cd_strip(_ptr(E), _ptr(I), _ptr(Kx), _ptr(Ky), Kx.shape[-1], N, W, erosion, dx, B, coeff, axis,
+                              L, A, _stream(stream), *[_ptr(t) for t in out]))
     return tuple(out)

@@ -80,3 +80,36 @@ def test_gpu_cd_after_training_forward(torch_cuda):
         _, _, ocd = O.measure_cd(np.stack(sig))
         assert np.all(np.isfinite(cd))
         assert np.abs(cd - ocd).max() < 0.01
+
+
+@pytest.mark.gpu
+def test_gpu_cd_strip_matches_full_pipeline(torch_cuda):
+    """CD from R on the measured line only (direct convolution) against the
+    full operator + CD, and against the FP64 oracle."""
+    torch = torch_cuda
+    import shrinkage_full_tests_b200 as srk
+    from tests.helpers import kernel
+    from tests.gpu_util import dev, spectra
+    for N, KW, B in ((256, 61, 6), (512, 121, 4)):
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        Kx, Ky = kernel(KW, "baseline", 4.0)
+        GX, GY = spectra(Kx, Ky, N, torch)
+        for axis, vertical in ((0, True), (1, False)):
+            imgs = [O.lns(vertical, N, s) for s in np.linspace(5.6, 11.2, B)]
+            E = torch.from_numpy(np.stack(imgs)).cuda()
+            R = torch.zeros((B, W, W), device="cuda")
+            plan = srk.SrkPlan(N, W, e, 4.0, B)
+            srk.srkTrainingForward(E, E, GX, GY, N, W, e, 4.0, B, None, R, plan)
+            _, _, cd_full = srk.cd_after_shrinkage(E, R, N, W, e, 0.3, axis)
+            _, _, cd_strip = srk.cd_strip(E, E, dev(Kx, torch), dev(Ky, torch), N, W, e, 4.0, 0.3, axis)
+            cd_full, cd_strip = cd_full.cpu().numpy(), cd_strip.cpu().numpy()
+            assert np.all(np.isfinite(cd_strip))
+            assert np.abs(cd_strip - cd_full).max() < 1e-3, (N, KW, axis)
+            sig = []
+            for b in range(B):
+                Ro = O.forward(imgs[b], imgs[b], Kx, Ky, e, 4.0)
+                s = imgs[b].astype(np.float64)[e:e + W, e:e + W] + 0.3 * Ro
+                sig.append(s[:, W // 2] if axis == 0 else s[W // 2, :])
+            _, _, ocd = O.measure_cd(np.stack(sig))
+            assert np.abs(cd_strip - ocd).max() < 0.01
