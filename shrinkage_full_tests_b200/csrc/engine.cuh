@@ -689,7 +689,45 @@ __device__ __forceinline__ void regs_to_row(float2* __restrict__ row, const floa
 }
 
 // P1: line `line` transforms column x = xb*LPU + line of every field along y.
-template <int M, int OP, typename T>
+// P1 output of one field: the line's transform z (ky = t + TPF*i) of
+// column xb*LPU + line -> S1.
+template <int M>
+__device__ __forceinline__ void p1_store(const float2 (&z)[M / tpf_of<M>()], float2* __restrict__ S1k, int xb,
+                                         float2* __restrict__ rows, int line, int t) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
+  constexpr int LPU = lpu_of<M>();
+  if constexpr (s1_blocked<M>()) {
+    // the unit's LPU columns -> shared tile of (ky/LPU) blocks -> whole
+    // LPU x LPU blocks of S1 (the staging rows are free after the transforms)
+    constexpr int PB = s2_block_pitch<M>();
+    constexpr int F4B = LPU * LPU / 2;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const int ky = t + TPF * i;
+      rows[(ky / LPU) * PB + line * LPU + (ky % LPU)] = z[i];
+    }
+    __syncthreads();
+    float2* dst = S1k + (size_t)xb * LPU * LPU;
+    for (int j = threadIdx.x; j < (M / LPU) * F4B; j += kThreads) {
+      const int q = j / F4B, v = j - (j / F4B) * F4B;
+      __stcg(reinterpret_cast<float4*>(dst + (size_t)q * M * LPU + 2 * v),
+             *reinterpret_cast<const float4*>(rows + q * PB + 2 * v));
+    }
+    __syncthreads();  // the rows are the next transform's exchange rows
+  } else {
+    float2* dst = S1k + (size_t)(xb * LPU + line) * M + t;
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) __stcg(dst + TPF * i, z[i]);
+  }
+}
+
+// P1: line `line` transforms column x = xb*LPU + line of every field along
+// y.  NU consecutive units (xb, xb+1, ...) per call, single-field ops only:
+// the next unit's columns are loaded before the current transform, so their
+// latency overlaps it.
+template <int M, int OP, typename T, int NU = 1>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t) {
   constexpr int TPF = tpf_of<M>();
@@ -697,36 +735,23 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
   constexpr int K = OpTraits<OP>::K;
   constexpr int LPU = lpu_of<M>();
   constexpr int RS = row_stride<M>();
-  const int x = xb * LPU + line;
+  static_assert(NU == 1 || (NU == 2 && K == 1), "two units per call for single-field ops only");
   float2* row = rows + line * RS;
+  if constexpr (NU == 2) {
+    float2 za[EPT], zb[EPT];
+    load_column<M, OP, T>(a, g, w, 0, xb * LPU + line, t, za);
+    load_column<M, OP, T>(a, g, w, 0, (xb + 1) * LPU + line, t, zb);
+    fft<M, false>(za, row, tw, t, 1 + line);
+    p1_store<M>(za, S1, xb, rows, line, t);
+    fft<M, false>(zb, row, tw, t, 1 + line);
+    p1_store<M>(zb, S1, xb + 1, rows, line, t);
+  } else {
 #pragma unroll 1
-  for (int k = 0; k < K; ++k) {
-    float2 z[EPT];
-    load_column<M, OP, T>(a, g, w, k, x, t, z);
-    fft<M, false>(z, row, tw, t, 1 + line);
-    if constexpr (s1_blocked<M>()) {
-      // the unit's LPU columns -> shared tile of (ky/LPU) blocks -> whole
-      // LPU x LPU blocks of S1 (the staging rows are free after the transforms)
-      constexpr int PB = s2_block_pitch<M>();
-      constexpr int F4B = LPU * LPU / 2;
-      __syncthreads();
-#pragma unroll
-      for (int i = 0; i < EPT; ++i) {
-        const int ky = t + TPF * i;
-        rows[(ky / LPU) * PB + line * LPU + (ky % LPU)] = z[i];
-      }
-      __syncthreads();
-      float2* dst = S1 + (size_t)k * M * M + (size_t)xb * LPU * LPU;
-      for (int j = threadIdx.x; j < (M / LPU) * F4B; j += kThreads) {
-        const int q = j / F4B, v = j - (j / F4B) * F4B;
-        __stcg(reinterpret_cast<float4*>(dst + (size_t)q * M * LPU + 2 * v),
-               *reinterpret_cast<const float4*>(rows + q * PB + 2 * v));
-      }
-      __syncthreads();  // the rows are the next field's exchange rows
-    } else {
-      float2* dst = S1 + ((size_t)k * M + x) * M + t;
-#pragma unroll
-      for (int i = 0; i < EPT; ++i) __stcg(dst + TPF * i, z[i]);
+    for (int k = 0; k < K; ++k) {
+      float2 z[EPT];
+      load_column<M, OP, T>(a, g, w, k, xb * LPU + line, t, z);
+      fft<M, false>(z, row, tw, t, 1 + line);
+      p1_store<M>(z, S1 + (size_t)k * M * M, xb, rows, line, t);
     }
   }
 }
@@ -991,6 +1016,13 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
 }
 
 // ---- three-launch schedule (one kernel per phase over a chunk of WTs) ------
+// Units per P1 CTA (see phase1): two for single-field ops (the second
+// unit's loads overlap the first transform; -4% at N=512), else one.
+#ifndef SRK_P1_UNITS
+#define SRK_P1_UNITS 2
+#endif
+template <int M, int OP>
+__host__ __device__ constexpr int p1_units() { return OpTraits<OP>::K == 1 ? SRK_P1_UNITS : 1; }
 template <int M, int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_P1_MIN_BLOCKS)
 k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
@@ -1000,8 +1032,9 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   load_twiddles(sm, twg, M);
   __syncthreads();
   const int wl = blockIdx.y;
-  phase1<M, OP, T>(a, g, w0 + wl, blockIdx.x, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(),
-                   sm, line, t);
+  constexpr int NU = p1_units<M, OP>();
+  phase1<M, OP, T, NU>(a, g, w0 + wl, blockIdx.x * NU, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(), sm,
+                       line, t);
 }
 
 template <int M, int OP>
