@@ -514,13 +514,19 @@ __device__ __forceinline__ void stage_grad_window_async(const T* __restrict__ im
     const T* col = img + (long long)(colin ? gx : 0) * N;
     T* d = dst + c * gw.HP;
     if (vec16) {
+      // chunk q of the column: rows gya + EPC*q ..; gya = gy0 - off >= 0, so
+      // a chunk is outside the image only past its last row (or off its columns)
       const int gya = gw.gy0 - gw.off;
       const int nch = (gw.off + gw.S + 2 + EPC - 1) / EPC;
-      for (int q = lane; q < nch; q += 32) {
-        const int gy = gya + EPC * q;
-        const bool in = colin && gy >= 0 && gy < N;
-        cp_async16_zfill(reinterpret_cast<float*>(d + EPC * q), reinterpret_cast<const float*>(in ? col + gy : img),
-                         in);
+      const int glim = colin ? N : -1;
+      const char* src = reinterpret_cast<const char*>(col + gya) + 16 * lane;
+      unsigned dsm = static_cast<unsigned>(__cvta_generic_to_shared(d)) + 16u * lane;
+      int gy = gya + EPC * lane;
+      for (int q = lane; q < nch; q += 32, src += 512, dsm += 512u, gy += 32 * EPC) {
+        const bool in = gy < glim;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dsm), "l"(in ? src : (const char*)img),
+                     "r"(in ? 16 : 0)
+                     : "memory");
       }
     } else if constexpr (std::is_same<T, float>::value) {
       for (int r = lane; r < gw.S + 2; r += 32) {
@@ -569,11 +575,12 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
     T* __restrict__ R = static_cast<T*>(a.out0);
     T* __restrict__ UX = static_cast<T*>(a.out_ux);
     T* __restrict__ UY = static_cast<T*>(a.out_uy);
-    if (R && !UX && !UY && vm == (1u << EPT) - 1u) {
-      // every row valid, R only: the common case
+    if (!UX && !UY) {
+      // R only (R is never NULL here): the common case
       T* __restrict__ Rp = R + ob;
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
+        if (!(vm >> i & 1u)) continue;
         const float2 z0i = z0s[RSP * i];
         const float ux = h ? z0i.y : z0i.x;
         const float uy = h ? z1[i].y : z1[i].x;
