@@ -310,13 +310,14 @@ __device__ __forceinline__ GradCol<T> grad_col(const T* f_img, int N, int e, int
 // Rows of this lane that carry valid outputs, as a bit mask over i.
 template <int M>
 __device__ __forceinline__ unsigned valid_rows(const Geom& g, const TileRef& t, int lane) {
-  unsigned m = 0;
-#pragma unroll
-  for (int i = 0; i < M / tpf_of<M>(); ++i) {
-    const int y = lane + tpf_of<M>() * i;
-    if (y >= g.e && y < g.e + g.S && t.y0 + y - g.e < t.Wout) m |= 1u << i;
-  }
-  return m;
+  // rows y = lane + TPF*i are valid for e <= y < yhi: a contiguous run of i
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
+  const int yhi = min(g.e + g.S, t.Wout - t.y0 + g.e);
+  const int ilo = max(0, (g.e - lane + TPF - 1) / TPF);        // first i with y >= e (g.e - lane > -TPF)
+  const int ihi = yhi - lane > 0 ? (yhi - lane + TPF - 1) / TPF : 0;  // first i with y >= yhi
+  const int hi = min(ihi, EPT);
+  return hi > ilo ? (((1u << hi) - 1u) & ~((1u << ilo) - 1u)) : 0u;
 }
 
 template <int M, int OP, typename T>
@@ -840,12 +841,12 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
       if (xv >= 0 && xv < S) tile[(xv / LPU) * PB + line * LPU + (xv % LPU)] = o[i];
     }
     __syncthreads();
-    float2* dst = S2 + ((size_t)l * nblk * M + ky0) * LPU;
-    for (int j = threadIdx.x; j < nblk * F4B; j += kThreads) {
-      const int q = j / F4B, w = j - (j / F4B) * F4B;
-      const float4 v = *reinterpret_cast<const float4*>(tile + q * PB + 2 * w);
-      __stcg(reinterpret_cast<float4*>(dst + (size_t)q * M * LPU + 2 * w), v);
-    }
+    // thread: value pair w of blocks q = q0, q0 + QS, ... (QS blocks per sweep)
+    constexpr int QS = kThreads / F4B;
+    const int q0 = threadIdx.x / F4B, w = threadIdx.x % F4B;
+    float4* dst = reinterpret_cast<float4*>(S2 + ((size_t)l * nblk * M + ky0) * LPU + (size_t)q0 * M * LPU + 2 * w);
+    const float4* src = reinterpret_cast<const float4*>(tile + q0 * PB + 2 * w);
+    for (int q = q0; q < nblk; q += QS, dst += (size_t)QS * M * LPU / 2, src += QS * PB / 2) __stcg(dst, *src);
     __syncthreads();  // the tile is reused by the next field
   };
   float2 z[EPT];
