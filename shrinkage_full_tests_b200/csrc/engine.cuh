@@ -775,18 +775,22 @@ __device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int p
   constexpr int Q = LPU / 2;                 // float4 per line
   constexpr int NIT = M * Q / kThreads;      // float4 loads per thread
   static_assert(M * Q % kThreads == 0, "staging loop must divide evenly");
+  // element j of this thread: line y0 + j*YS, value pair cp (YS is a multiple
+  // of 16, so fft_pad(y0 + j*YS) = fft_pad(y0) + fft_pad(j*YS))
+  constexpr int YS = kThreads / Q;
+  static_assert(YS % 16 == 0, "line step must keep the padding separable");
+  const int y0 = threadIdx.x / Q, cp = threadIdx.x % Q;
+  const float4* sp = reinterpret_cast<const float4*>(src + (size_t)y0 * pitch + 2 * cp);
+  const size_t sstep = (size_t)YS * pitch / 2;  // float4 per j (pitch is even)
   float4 q[NIT];
 #pragma unroll
-  for (int j = 0; j < NIT; ++j) {
-    const int idx = threadIdx.x + j * kThreads;
-    q[j] = __ldcg(reinterpret_cast<const float4*>(src + (size_t)(idx / Q) * pitch + 2 * (idx % Q)));
-  }
+  for (int j = 0; j < NIT; ++j) q[j] = __ldcg(sp + j * sstep);
+  float2* r0 = rows + (2 * cp) * RS + fft_pad(y0);
+  float2* r1 = r0 + RS;
 #pragma unroll
   for (int j = 0; j < NIT; ++j) {
-    const int idx = threadIdx.x + j * kThreads;
-    const int y = idx / Q, cp = idx % Q;
-    rows[(2 * cp) * RS + fft_pad(y)] = make_float2(q[j].x, q[j].y);
-    rows[(2 * cp + 1) * RS + fft_pad(y)] = make_float2(q[j].z, q[j].w);
+    r0[fft_pad(j * YS)] = make_float2(q[j].x, q[j].y);
+    r1[fft_pad(j * YS)] = make_float2(q[j].z, q[j].w);
   }
 }
 
