@@ -212,6 +212,33 @@ srk_status srk_tangent_adjoint_ragged(const float* d_f, const float* d_g, const 
                                       const void* d_Gy_freq, int B, const int* Ns, int erosion, float dx,
                                       srk_stream_t stream, float* d_dLam_f, float* d_dLam_g, srk_plan plan);
 
+/* ---- column slabs of one image ----------------------------------------------
+ * One N x N image split by columns (contiguous runs in the column-major
+ * layout), e.g. across GPUs.  These compute the output columns [c0, c1) of
+ * srkForwardOaS / shrinkageTangentOaS (columns of the W x W output) or of
+ * adjointSRK (columns of the N x N outputs).  Every pointer addresses column
+ * c0 of its array; the buffer behind it must hold these columns (clipped to
+ * the array):
+ *   forward, tangent: N-sized inputs columns [c0, c1 + 2*erosion); R / dh [c0, c1).
+ *   adjoint: v, ux, uy (W-sized) columns [c0 - 2*erosion, c1); I columns
+ *            [c0 - erosion - 1, c1 + erosion + 1); dLdI, dLdE [c0, c1).
+ * c1 - c0 must be a multiple of the plan's tile_stride (srk_plan_get_info)
+ * unless c1 is the last output column (W, or N for the adjoint).  The plan
+ * is one made for the whole image (N <= its N).  The reference has no slab
+ * form; these replace srkForwardOaS (srk_forward.cuh:468-501),
+ * shrinkageTangentOaS (srk_tangent.cuh:111-151) and adjointSRK
+ * (srk_adjoint.cuh:402-425) on one slab. */
+srk_status srk_forward_oas_slab(const float* d_E, const float* d_I, const void* d_Gx_freq,
+                                const void* d_Gy_freq, int N, int erosion, float dx, int c0, int c1,
+                                srk_stream_t stream, float* d_R, srk_plan plan);
+srk_status srk_tangent_slab(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                            const void* d_Gx_freq, const void* d_Gy_freq, int N, int erosion, float dx,
+                            int c0, int c1, srk_stream_t stream, float* d_dh, srk_plan plan);
+srk_status srk_adjoint_slab(const float* d_v, const float* d_ux, const float* d_uy, const float* d_I,
+                            const void* d_Gx_freq, const void* d_Gy_freq, int N, int erosion, float dx,
+                            int c0, int c1, srk_stream_t stream, float* d_dLdI, float* d_dLdE,
+                            srk_plan plan);
+
 /* ---- synthetic inputs on the device -----------------------------------------
  * Gaussian random fields as GpGenerator (third_party/include/stTestCore/
  * gp_generator.h:95-254): white N(0,1) noise on the Np x Np grid (Np = next

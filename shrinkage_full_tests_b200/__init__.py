@@ -94,6 +94,9 @@ _SIGS = {
     "srk_adjoint_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P, _P],
     "srk_tangent_ragged": [_P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P],
     "srk_tangent_adjoint_ragged": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _P, _I, _F, _P, _P, _P, _P],
+    "srk_forward_oas_slab": [_P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P],
+    "srk_tangent_slab": [_P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P],
+    "srk_adjoint_slab": [_P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P, _P],
 }
 # storage-typed forms (void* buffers in the plan's dtype): same argument types
 for _n in ("srk_training_forward", "srk_forward_oas", "srk_adjoint", "srk_tangent", "srk_tangent_adjoint",
@@ -274,6 +277,24 @@ def shrinkageTangentAdjointOaSRagged(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_fr
     _check(lib().srk_tangent_adjoint_ragged(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
                                             _ptr(Gx_freq), _ptr(Gy_freq), B, arr, erosion, dx, _stream(stream),
                                             _ptr(dLam_f), _ptr(dLam_g), ws.handle))
+
+
+# ---- column slabs of one image: every tensor's data pointer addresses column
+# c0 of its array (a view such as buf[k:] of a halo'd column buffer), with the
+# halo columns of the C declarations readable around it
+def srkForwardOaSSlab(E, I, Gx_freq, Gy_freq, N, erosion, dx, c0, c1, stream, R, ws):
+    _check(lib().srk_forward_oas_slab(_ptr(E), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, erosion, dx, c0, c1,
+                                      _stream(stream), _ptr(R), ws.handle))
+
+
+def shrinkageTangentOaSSlab(f, g, df, dg, Gx_freq, Gy_freq, N, erosion, dx, c0, c1, stream, dh, ws):
+    _check(lib().srk_tangent_slab(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(Gx_freq), _ptr(Gy_freq), N, erosion,
+                                  dx, c0, c1, _stream(stream), _ptr(dh), ws.handle))
+
+
+def adjointSRKSlab(v, ux, uy, I, Gx_freq, Gy_freq, N, erosion, dx, c0, c1, stream, dLdI, dLdE, ws):
+    _check(lib().srk_adjoint_slab(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, erosion,
+                                  dx, c0, c1, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
 
 
 # ---- synthetic inputs on the device

@@ -72,11 +72,15 @@ template <> struct OpTraits<OP_TANADJ_F> { static constexpr int K = 1, L = 2; st
 template <> struct OpTraits<OP_ADJ>      { static constexpr int K = 2, L = 1; static constexpr bool PAIRS = true; };
 
 // One image of a ragged batch: its size and where it starts in the
-// concatenated N-sized and W-sized batch arrays (elements).
+// concatenated N-sized and W-sized batch arrays (elements).  A column slab
+// of one image is a one-image table whose offsets are negative (the
+// caller's pointers address the slab's first column) and whose stencil
+// blocks cover only the pixel columns [cx0, cx1).
 struct RagImage {
   long long on, ow;
   int N, W;
-  int blk0;  // first block of this image in the ragged stencil launch
+  int blk0;      // first block of this image in the ragged stencil launch
+  int cx0, cx1;  // pixel columns of the N x N output the stencil writes
   int pad;
 };
 
@@ -1260,8 +1264,8 @@ __global__ void k_adj_wrt_f_rag(const float* __restrict__ wx, const float* __res
   const int nby = (N + 31) / 32;
   const int k = blk - im.blk0;
   const int gy = (k % nby) * 32 + threadIdx.x;
-  const int gx = (k / nby) * 8 + threadIdx.y;
-  if (gx >= N || gy >= N) return;
+  const int gx = im.cx0 + (k / nby) * 8 + threadIdx.y;
+  if (gx >= im.cx1 || gy >= N) return;
   auto WX = [&](int r, int c) -> float {
     if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
     const long long i = im.ow + (long long)c * W + r;

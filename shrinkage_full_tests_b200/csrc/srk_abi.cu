@@ -698,6 +698,43 @@ srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, 
 }
 
 // ---- ragged batches -----------------------------------------------------------
+// Uploads the tile tables of the forward-type (`fwd`) and adjoint-type
+// (`adj`) geometries and the image table, keyed by `key` (the sizes of a
+// ragged batch, or a slab's image and columns).
+srk_status upload_tables(srk_plan_s* p, std::vector<int> key, std::vector<int4> fwd, const std::vector<int4>& adj,
+                         const std::vector<RagImage>& imgs, int nblk, long long sum_nn, long long sum_ww,
+                         cudaStream_t s) {
+  const size_t nt = fwd.size() + adj.size();
+  const size_t B = imgs.size();
+  if (p->rag_tiles_cap < nt) {
+    if (p->rag_tiles) SRK_CUDA(cudaFreeAsync(p->rag_tiles, s));
+    p->rag_tiles = nullptr;
+    p->rag_tiles_cap = 0;
+    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_tiles), nt * sizeof(int4), s));
+    p->rag_tiles_cap = nt;
+  }
+  if (p->rag_imgs_cap < B) {
+    if (p->rag_imgs) SRK_CUDA(cudaFreeAsync(p->rag_imgs, s));
+    p->rag_imgs = nullptr;
+    p->rag_imgs_cap = 0;
+    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_imgs), B * sizeof(RagImage), s));
+    p->rag_imgs_cap = B;
+  }
+  const int nfwd = (int)fwd.size();
+  fwd.insert(fwd.end(), adj.begin(), adj.end());
+  // pageable sources: the copies have taken the data when the calls return
+  SRK_CUDA(cudaMemcpyAsync(p->rag_tiles, fwd.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, s));
+  SRK_CUDA(cudaMemcpyAsync(p->rag_imgs, imgs.data(), B * sizeof(RagImage), cudaMemcpyHostToDevice, s));
+  p->rag_key = std::move(key);
+  p->rag_ntiles_fwd = nfwd;
+  p->rag_ntiles_adj = (int)adj.size();
+  p->rag_nblk = nblk;
+  p->rag_sum_nn = sum_nn;
+  p->rag_sum_ww = sum_ww;
+  return SRK_OK;
+}
+
+
 // B images of sizes Ns[b] (each 2*erosion+1 <= N_b <= the plan's N; same
 // erosion, dx, tile size and spectra), concatenated column-major in every
 // buffer: N-sized arrays hold N_b^2 elements per image, W-sized ones W_b^2.
@@ -723,6 +760,8 @@ srk_status ragged_tables(srk_plan_s* p, int B, const int* Ns, cudaStream_t s) {
     imgs[b].N = N;
     imgs[b].W = W;
     imgs[b].blk0 = (int)blk;
+    imgs[b].cx0 = 0;
+    imgs[b].cx1 = N;
     imgs[b].pad = 0;
     on += (long long)N * N;
     ow += (long long)W * W;
@@ -735,32 +774,43 @@ srk_status ragged_tables(srk_plan_s* p, int B, const int* Ns, cudaStream_t s) {
   }
   if (blk > (1ll << 30) || fwd.size() + adj.size() > (1u << 30))
     return fail(SRK_ERR_UNSUPPORTED, "ragged batch too large (%lld pixel blocks)", blk);
-  const size_t nt = fwd.size() + adj.size();
-  if (p->rag_tiles_cap < nt) {
-    if (p->rag_tiles) SRK_CUDA(cudaFreeAsync(p->rag_tiles, s));
-    p->rag_tiles = nullptr;
-    p->rag_tiles_cap = 0;
-    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_tiles), nt * sizeof(int4), s));
-    p->rag_tiles_cap = nt;
-  }
-  if (p->rag_imgs_cap < (size_t)B) {
-    if (p->rag_imgs) SRK_CUDA(cudaFreeAsync(p->rag_imgs, s));
-    p->rag_imgs = nullptr;
-    p->rag_imgs_cap = 0;
-    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_imgs), (size_t)B * sizeof(RagImage), s));
-    p->rag_imgs_cap = B;
-  }
-  fwd.insert(fwd.end(), adj.begin(), adj.end());
-  // pageable sources: the copies have taken the data when the calls return
-  SRK_CUDA(cudaMemcpyAsync(p->rag_tiles, fwd.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, s));
-  SRK_CUDA(cudaMemcpyAsync(p->rag_imgs, imgs.data(), (size_t)B * sizeof(RagImage), cudaMemcpyHostToDevice, s));
-  p->rag_key = key;
-  p->rag_ntiles_fwd = (int)(nt - adj.size());
-  p->rag_ntiles_adj = (int)adj.size();
-  p->rag_nblk = (int)blk;
-  p->rag_sum_nn = on;
-  p->rag_sum_ww = ow;
-  return SRK_OK;
+  return upload_tables(p, std::move(key), std::move(fwd), adj, imgs, (int)blk, on, ow, s);
+}
+
+// Column slab [c0, c1) of one N x N image.  Output columns of the
+// forward-type geometry (W x W) or, with `adj`, of the adjoint-type one
+// (N x N); the tiles start at c0 and step by the tile stride S, so the slab
+// spans whole tiles unless it ends at the last output column.  The caller's
+// pointers address the slab's first column (column c0 of every array), so
+// the image offsets are -c0 columns.
+srk_status slab_tables(srk_plan_s* p, int N, int c0, int c1, bool adj, cudaStream_t s) {
+  const int e = p->e, S = p->S, W = N - 2 * e;
+  if (N < 2 * e + 1 || N > p->N)
+    return fail(SRK_ERR_INVALID_ARG, "slab image N=%d outside [2*erosion+1=%d, plan N=%d]", N, 2 * e + 1, p->N);
+  const int Wo = adj ? N : W;
+  if (c0 < 0 || c1 <= c0 || c1 > Wo)
+    return fail(SRK_ERR_INVALID_ARG, "slab columns [%d, %d) outside [0, %d)", c0, c1, Wo);
+  if ((c1 - c0) % S != 0 && c1 != Wo)
+    return fail(SRK_ERR_INVALID_ARG, "slab [%d, %d) must span whole tiles of %d columns or end at column %d", c0, c1,
+                S, Wo);
+  std::vector<int> key = {adj ? -2 : -1, N, c0, c1};
+  if (key == p->rag_key) return SRK_OK;
+  std::vector<int4> tiles;
+  for (int x0 = c0; x0 < c1; x0 += S)
+    for (int y0 = 0; y0 < Wo; y0 += S) tiles.push_back(make_int4(0, x0, y0, 0));
+  std::vector<RagImage> imgs(1);
+  imgs[0].on = -(long long)c0 * N;
+  imgs[0].ow = -(long long)c0 * W;
+  imgs[0].N = N;
+  imgs[0].W = W;
+  imgs[0].blk0 = 0;
+  imgs[0].cx0 = adj ? c0 : 0;
+  imgs[0].cx1 = adj ? c1 : 0;
+  imgs[0].pad = 0;
+  const int nblk = adj ? ((N + 31) / 32) * ((c1 - c0 + 7) / 8) : 0;
+  std::vector<int4> none;
+  return adj ? upload_tables(p, std::move(key), std::move(none), tiles, imgs, nblk, 0, 0, s)
+             : upload_tables(p, std::move(key), std::move(tiles), none, imgs, nblk, 0, 0, s);
 }
 
 Geom ragged_geom(const srk_plan_s* p, bool adj) {
@@ -881,6 +931,60 @@ srk_status op_tangent_adjoint_ragged(const void* f, const void* g, const void* d
   return launch_conv_dt<OP_ADJ>(p, b, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
 }
 
+// ---- column slabs of one image ------------------------------------------------
+srk_status op_forward_oas_slab(const void* E, const void* I, const void* gx, const void* gy, int N, int erosion,
+                               float dx, int c0, int c1, srk_stream_t s, void* R, srk_plan p) {
+  const NvtxRange nvtx_range("srk_forward_oas_slab");
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(E);
+  SRK_NONNULL(I);
+  SRK_NONNULL(R);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(slab_tables(p, N, c0, c1, false, s));
+  OpArgs a = base_args(p);
+  a.E = E; a.I = I; a.out0 = R;
+  return launch_conv_dt<OP_FWD>(p, a, ragged_geom(p, false), false, s);
+}
+
+srk_status op_tangent_slab(const void* f, const void* g, const void* df, const void* dg, const void* gx,
+                           const void* gy, int N, int erosion, float dx, int c0, int c1, srk_stream_t s, void* dh,
+                           srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent_slab");
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(f);
+  SRK_NONNULL(g);
+  SRK_NONNULL(df);
+  SRK_NONNULL(dg);
+  SRK_NONNULL(dh);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(slab_tables(p, N, c0, c1, false, s));
+  OpArgs a = base_args(p);
+  a.E = g; a.dE = dg; a.I = f; a.dI = df; a.out0 = dh;
+  return launch_conv_dt<OP_JVP>(p, a, ragged_geom(p, false), false, s);
+}
+
+srk_status op_adjoint_slab(const void* v, const void* ux, const void* uy, const void* I, const void* gx,
+                           const void* gy, int N, int erosion, float dx, int c0, int c1, srk_stream_t s, void* dLdI,
+                           void* dLdE, srk_plan p) {
+  const NvtxRange nvtx_range("srk_adjoint_slab");
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(v);
+  SRK_NONNULL(ux);
+  SRK_NONNULL(uy);
+  SRK_NONNULL(I);
+  SRK_NONNULL(dLdI);
+  SRK_NONNULL(dLdE);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  SRK_TRY(slab_tables(p, N, c0, c1, true, s));
+  SRK_TRY(adj_wrt_f_rag(p, nullptr, nullptr, v, ux, uy, 1, dLdI, s));
+  OpArgs a = base_args(p);
+  a.v = v; a.I = I; a.out0 = dLdE;
+  return launch_conv_dt<OP_ADJ>(p, a, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
+}
+
 // The float* entry points are the reference drop-ins: fp32 plans only.
 srk_status need_f32(srk_plan p) {
   if (p && p->dtype != SRK_F32)
@@ -945,6 +1049,26 @@ srk_status srk_jvp(const float* f, const float* g, const float* df, const float*
                    float* dh, srk_plan p) {
   SRK_TRY(need_f32(p));
   return op_jvp(f, g, df, dg, B, s, dh, p);
+}
+
+srk_status srk_forward_oas_slab(const float* E, const float* I, const void* gx, const void* gy, int N, int erosion,
+                                float dx, int c0, int c1, srk_stream_t s, float* R, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_forward_oas_slab(E, I, gx, gy, N, erosion, dx, c0, c1, s, R, p);
+}
+
+srk_status srk_tangent_slab(const float* f, const float* g, const float* df, const float* dg, const void* gx,
+                            const void* gy, int N, int erosion, float dx, int c0, int c1, srk_stream_t s, float* dh,
+                            srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent_slab(f, g, df, dg, gx, gy, N, erosion, dx, c0, c1, s, dh, p);
+}
+
+srk_status srk_adjoint_slab(const float* v, const float* ux, const float* uy, const float* I, const void* gx,
+                            const void* gy, int N, int erosion, float dx, int c0, int c1, srk_stream_t s,
+                            float* dLdI, float* dLdE, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_adjoint_slab(v, ux, uy, I, gx, gy, N, erosion, dx, c0, c1, s, dLdI, dLdE, p);
 }
 
 srk_status srk_forward_oas_ragged(const float* E, const float* I, const void* gx, const void* gy, int B,
