@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--no-ops", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the fp16 and published-config lines")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--large-slabs", action="store_true",
+                   help="also time one N=32768 KW=121 image split by column slabs over the ranks "
+                        "(halo exchange + slab forward / adjoint)")
     p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass"],
                    help="override the autotuned kernel schedule (profiling)")
     p.add_argument("--tile-M", type=int, default=0,
@@ -303,6 +306,10 @@ def run_ours(a):
         extra["large_image"] = ops_throughput(torch, srk, N=32768, KW=121, reps=1, spectra_M=2048, ell=32.0)
         torch.cuda.empty_cache()
 
+    if a.large_slabs:
+        extra["large_image_slabs"] = large_image_slabs(torch, srk, rank, world, dist)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         nth = os.cpu_count() or 1
@@ -406,6 +413,34 @@ def ops_throughput(torch, srk, N=4096, KW=61, reps=3, spectra_M=1024, ell=8.0):
         px = W * W if k in ("forward", "tangent") else N * N
         out[k] = {"ms": ms, "out_mpix_per_s": px / (ms * 1e-3) / 1e6,
                   "hbm_frac": alg[k] * 4 / (ms * 1e-3) / 1e9 / peak}
+    return out
+
+
+def large_image_slabs(torch, srk, rank, world, dist, N=32768, KW=121, reps=2, spectra_M=2048):
+    """One N x N image split by column slabs over the ranks: each rank holds
+    its own columns, exchanges the halos with its neighbours (NCCL
+    point-to-point) and computes its output columns; the time of each op is
+    the max over ranks of exchange + slab launch sequence."""
+    from shrinkage_full_tests_b200 import shard
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    _, _, GX, GY = make_spectra(torch, srk, KW, spectra_M, 1.0)
+    plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=spectra_M, tile_M=512)
+    S = plan.info()["tile_stride"]
+    lo, hi = shard.slab_bounds(N, e, S, world)[rank]
+    wlo, whi = min(lo, W), min(hi, W)
+    gen = torch.Generator(device="cuda").manual_seed(5 + rank)
+    f, g = (torch.rand((hi - lo, N), device="cuda", generator=gen) for _ in range(2))
+    v, ux, uy = (torch.randn((whi - wlo, W), device="cuda", generator=gen) for _ in range(3))
+    fwd, _, adj = shard.device_slab_ops(plan, GX, GY, N, e, 1.0)
+    runs = {"forward": lambda: shard.forward_slabs(g, f, N, e, S, rank, world, dist, fwd),
+            "adjoint": lambda: shard.adjoint_slabs(v, ux, uy, f, N, e, S, rank, world, dist, adj)}
+    out = {"config": "N=%d KW=%d one image over %d GPU(s), column slabs of whole %d-column tiles" % (N, KW, world, S),
+           "slab_columns_rank0": list(shard.slab_bounds(N, e, S, world)[0])}
+    for k, fn in runs.items():
+        ms = max_over_ranks(torch, dist, time_steps(torch, fn, reps, 1, dist))
+        px = W * W if k == "forward" else N * N
+        out[k] = {"ms": ms, "out_mpix_per_s": px / (ms * 1e-3) / 1e6}
     return out
 
 
