@@ -74,7 +74,8 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   for (int w0 = 0; w0 < nwt; w0 += chunk) {
     const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
     constexpr int LPU = lpu_of<M>();
-    k_p1<M, OP, T><<<dim3(M / LPU / p1_units<M, OP>(), c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S);
+    k_p1<M, OP, T><<<dim3(M / LPU / p1_units<M, OP>(), c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S,
+                                                                                 p->nsm);
     k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
     k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
     launches += 3;

@@ -735,13 +735,35 @@ __device__ __forceinline__ void p1_store(const float2 (&z)[M / tpf_of<M>()], flo
   }
 }
 
+// L2 prefetch of the image columns that P1 units xb2 .. xb2+NU-1 of WT w2
+// load (single-field ops: the two tiles of a pair, or E and dE of one
+// tile).  One 128-byte line per thread; only addresses inside the images.
+template <int M, int OP, typename T, int NU>
+__device__ __forceinline__ void p1_prefetch(const OpArgs& a, const Geom& g, int w2, int xb2) {
+  constexpr int C = lpu_of<M>() * NU;                     // columns per field
+  constexpr int RPL = 128 / (int)sizeof(T);              // rows per line
+  constexpr int LC = (M + RPL - 1) / RPL;                 // lines per column
+  static_assert(C * LC <= kThreads / 2, "one line per thread and field");
+  const int h = threadIdx.x / (kThreads / 2), r = threadIdx.x % (kThreads / 2);
+  if (r >= C * LC) return;
+  const TileRef tr = OpTraits<OP>::PAIRS ? tile_of(g, 2 * w2 + h) : tile_of(g, w2);
+  const int gx = tr.x0 + xb2 * lpu_of<M>() + r / LC;
+  const int gy = tr.y0 + (r % LC) * RPL;
+  if (!tr.live || gx >= tr.N || gy >= tr.N) return;
+  const T* img = static_cast<const T*>(OpTraits<OP>::PAIRS || h == 0 ? a.E : a.dE);
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(img + tr.on + (long long)gx * tr.N + gy));
+}
+
 // P1: line `line` transforms column x = xb*LPU + line of every field along
 // y.  NU consecutive units (xb, xb+1, ...) per call, single-field ops only:
 // the next unit's columns are loaded before the current transform, so their
-// latency overlaps it.
+// latency overlaps it, and the columns of the CTA `ahead` launch positions
+// later (about one per SM: it starts when this one is nearly done) are
+// prefetched into L2.
 template <int M, int OP, typename T, int NU = 1>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
-                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t) {
+                                       float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
+                                       int ahead = 0) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int K = OpTraits<OP>::K;
@@ -750,6 +772,10 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
   static_assert(NU == 1 || (NU == 2 && K == 1), "two units per call for single-field ops only");
   float2* row = rows + line * RS;
   if constexpr (NU == 2) {
+    if (ahead > 0) {
+      const int lin = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
+      p1_prefetch<M, OP, T, NU>(a, g, w - (int)blockIdx.y + lin / (int)gridDim.x, (lin % (int)gridDim.x) * NU);
+    }
     float2 za[EPT], zb[EPT];
     load_column<M, OP, T>(a, g, w, 0, xb * LPU + line, t, za);
     load_column<M, OP, T>(a, g, w, 0, (xb + 1) * LPU + line, t, zb);
@@ -1041,7 +1067,7 @@ template <int M, int OP>
 __host__ __device__ constexpr int p1_units() { return OpTraits<OP>::K == 1 ? SRK_P1_UNITS : 1; }
 template <int M, int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_P1_MIN_BLOCKS)
-k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S) {
+k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S, int ahead) {
   extern __shared__ float2 sm[];
   constexpr int TPF = tpf_of<M>();
   const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
@@ -1050,7 +1076,7 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   const int wl = blockIdx.y;
   constexpr int NU = p1_units<M, OP>();
   phase1<M, OP, T, NU>(a, g, w0 + wl, blockIdx.x * NU, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(), sm,
-                       line, t);
+                       line, t, ahead);
 }
 
 template <int M, int OP>

@@ -56,6 +56,7 @@ inline srk_status cuda_status(cudaError_t e, const char* what) {
 
 struct srk_plan_s {
   int device = 0;
+  int nsm = 0;  // SMs of the device (P1's L2 prefetch distance)
   int N = 0, W = 0, e = 0, B_max = 0, spectra_M = 0;
   float dx = 1.f;
   srk_dtype dtype = SRK_F32;

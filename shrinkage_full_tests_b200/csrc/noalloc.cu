@@ -119,6 +119,7 @@ extern "C" srk_status srk_training_forward_noalloc(const float* d_E, const float
   // A plan view over the static array (host struct on the stack; nothing is allocated).
   srk_plan_s view;
   cudaGetDevice(&view.device);
+  cudaDeviceGetAttribute(&view.nsm, cudaDevAttrMultiProcessorCount, view.device);
   view.N = N; view.W = W; view.e = erosion; view.dx = dx; view.B_max = B; view.spectra_M = N;
   view.dtype = SRK_F32;
   view.M = M; view.S = S; view.T = 1; view.Ta = 1;

@@ -369,6 +369,7 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
 
   srk_plan_s* p = new srk_plan_s();
   cudaGetDevice(&p->device);
+  cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
   p->N = N; p->W = W; p->e = erosion; p->dx = dx; p->B_max = B_max; p->spectra_M = spectra_M; p->dtype = dtype;
   p->M = M; p->S = M - 2 * erosion;
   p->schedule = sched;
