@@ -70,13 +70,33 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   SRK_TRY(set_smem(k_p2<M, OP>, sm2));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
   const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
+  // With several chunks, P1 of chunk k+1 (writes S1) runs on the side
+  // stream next to P3 of chunk k (reads S2): it waits for P2 of chunk k
+  // (the last reader of S1), and P2 of chunk k+1 waits for it and, by the
+  // order of s, for P3 of chunk k (the last reader of S2).  The side stream
+  // is joined back into s by the wait before the last P2.
+  const bool ovl = p->overlap && p->side && nwt > chunk;
+  if (ovl) {
+    SRK_CUDA(cudaEventRecord(p->ev_fork, s));
+    SRK_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+  }
   int launches = 0;
   for (int w0 = 0; w0 < nwt; w0 += chunk) {
     const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
     constexpr int LPU = lpu_of<M>();
-    k_p1<M, OP, T><<<dim3(M / LPU / p1_units<M, OP>(), c), kThreads, sm1, s>>>(a, g, p->tw, w0, p->scratch, g.S,
-                                                                                 p->nsm);
+    cudaStream_t s1 = s;
+    if (ovl) {
+      s1 = p->side;
+      if (w0 > 0) SRK_CUDA(cudaStreamWaitEvent(s1, p->ev_p2, 0));
+    }
+    k_p1<M, OP, T><<<dim3(M / LPU / p1_units<M, OP>(), c), kThreads, sm1, s1>>>(a, g, p->tw, w0, p->scratch, g.S,
+                                                                                  p->nsm);
+    if (ovl) {
+      SRK_CUDA(cudaEventRecord(p->ev_p1, s1));
+      SRK_CUDA(cudaStreamWaitEvent(s, p->ev_p1, 0));
+    }
     k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
+    if (ovl) SRK_CUDA(cudaEventRecord(p->ev_p2, s));
     k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
     launches += 3;
   }

@@ -81,6 +81,11 @@ struct srk_plan_s {
   unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
   int persist_lag = 0, persist_grid = 0, persist_prefetch = 0;
   int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
+  // three-pass schedule: P1 of chunk k+1 runs on a side stream while P3 of
+  // chunk k finishes (S1 and S2 are separate regions of the scratch)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_p1 = nullptr, ev_p2 = nullptr;
+  bool overlap = true;
   // ragged batches: device tables of the last ragged call (tile -> image,
   // per-image sizes/offsets), rebuilt only when the image sizes change
   int4* rag_tiles = nullptr;
