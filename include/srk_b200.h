@@ -35,7 +35,7 @@ typedef struct srk_plan_s* srk_plan;
 typedef enum srk_status {
   SRK_OK = 0,
   SRK_ERR_INVALID_ARG = 1, /* bad size / null pointer / mismatch with the plan */
-  SRK_ERR_UNSUPPORTED = 2, /* valid request this build cannot serve (e.g. tile too small) */
+  SRK_ERR_UNSUPPORTED = 2, /* valid request the library cannot serve (e.g. tile too small) */
   SRK_ERR_ALLOC = 3,       /* device allocation failed */
   SRK_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
   SRK_ERR_CUDA = 5         /* a CUDA runtime call failed */
