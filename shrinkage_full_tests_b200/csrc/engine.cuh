@@ -272,6 +272,59 @@ __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int 
   }
 }
 
+// Both adjoint-type fields of one P1 column at once (erosion >= 1, so every
+// gradient neighbour of the valid window lies inside the image): zx = h_x,
+// zy = h_y of the two tiles of WT w (re / im) at virtual column x, rows
+// lane + TPF i.  Per element one load of v (and dv) and the four neighbours
+// of f (and df), shared by h_x and h_y; the arithmetic is h_at's.
+template <int M, typename T>
+__device__ __forceinline__ void load_adj_column(const OpArgs& a, const Geom& g, int w, int x, int lane,
+                                                float2 (&zx)[M / tpf_of<M>()], float2 (&zy)[M / tpf_of<M>()]) {
+  constexpr int TPF = tpf_of<M>();
+  constexpr int EPT = M / TPF;
+#pragma unroll
+  for (int i = 0; i < EPT; ++i) zx[i] = zy[i] = make_float2(0.f, 0.f);
+  const bool tan = a.dI != nullptr;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const TileRef tr = tile_of(g, 2 * w + h);
+    const int qx = tr.x0 + x - a.e, ox = qx - a.e;  // image / valid-window column
+    if (!tr.live || ox < 0 || ox >= tr.W) continue;
+    const int qy0 = tr.y0 + lane - a.e, oy0 = qy0 - a.e;
+    const long long vo = tr.ow + (long long)ox * tr.W + oy0;
+    const long long fo = tr.on + (long long)qx * tr.N + qy0;
+    const T* vc = static_cast<const T*>(a.v) + vo;
+    const T* fc = static_cast<const T*>(a.I) + fo;
+    const T* dvc = tan ? static_cast<const T*>(a.dv) + vo : vc;
+    const T* dfc = tan ? static_cast<const T*>(a.dI) + fo : fc;
+    const int N = tr.N;
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+      const bool in = (unsigned)(oy0 + TPF * i) < (unsigned)tr.W;
+      const int o = TPF * i;
+      const float v = in ? ldf(vc, o) : 0.f;
+      const float gx = ((in ? ldf(fc + N, o) : 0.f) - (in ? ldf(fc - N, o) : 0.f)) * 0.5f;
+      const float gy = ((in ? ldf(fc + 1, o) : 0.f) - (in ? ldf(fc - 1, o) : 0.f)) * 0.5f;
+      float hx = v * gx, hy = v * gy;
+      if (tan) {
+        const float dv = in ? ldf(dvc, o) : 0.f;
+        const float dgx = ((in ? ldf(dfc + N, o) : 0.f) - (in ? ldf(dfc - N, o) : 0.f)) * 0.5f;
+        const float dgy = ((in ? ldf(dfc + 1, o) : 0.f) - (in ? ldf(dfc - 1, o) : 0.f)) * 0.5f;
+        hx = dot2(dv, gx, v, dgx);
+        hy = dot2(dv, gy, v, dgy);
+      }
+      if (!in) hx = hy = 0.f;
+      if (h == 0) {
+        zx[i].x = hx;
+        zy[i].x = hy;
+      } else {
+        zx[i].y = hx;
+        zy[i].y = hy;
+      }
+    }
+  }
+}
+
 // Central differences of f at image column gx for this lane's rows
 // gy = gy0 + 32 i: fx = (f[gx+1] - f[gx-1])/2, fy = (f[gy+1] - f[gy-1])/2.
 // With erosion >= 1 every valid output has its 4 neighbours inside the
@@ -683,6 +736,11 @@ __host__ __device__ inline size_t wt_elems(int S) {
 // (P2 adds its block tile, P3 its first gradient window).
 template <int M>
 constexpr size_t phase_smem_bytes() { return sizeof(float2) * (tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()); }
+// P1 of the adjoint-type op adds the stash of the second field.
+template <int M, int OP>
+constexpr size_t p1_smem_bytes() {
+  return phase_smem_bytes<M>() + (OP == OP_ADJ ? sizeof(float2) * kThreads * (M / tpf_of<M>()) : 0);
+}
 
 // Copies between a thread's registers (strided order) and a padded row.
 template <int M>
@@ -763,7 +821,7 @@ __device__ __forceinline__ void p1_prefetch(const OpArgs& a, const Geom& g, int 
 template <int M, int OP, typename T, int NU = 1>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
-                                       int ahead = 0) {
+                                       int ahead = 0, float2* __restrict__ stash = nullptr) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
   constexpr int K = OpTraits<OP>::K;
@@ -784,6 +842,24 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
     fft<M, false>(zb, row, tw, t, 1 + line);
     p1_store<M>(zb, S1, xb + 1, rows, line, t);
   } else {
+    if constexpr (OP == OP_ADJ) {
+      // both fields from one pass over the inputs; h_y waits in the
+      // stash (kThreads x EPT values after the rows, each thread its own)
+      if (stash && a.e >= 1) {
+        float2 zx[EPT], zy[EPT];
+        load_adj_column<M, T>(a, g, w, xb * LPU + line, t, zx, zy);
+        float2* st = stash + threadIdx.x;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) st[kThreads * i] = zy[i];
+        fft<M, false>(zx, row, tw, t, 1 + line);
+        p1_store<M>(zx, S1, xb, rows, line, t);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) zx[i] = st[kThreads * i];
+        fft<M, false>(zx, row, tw, t, 1 + line);
+        p1_store<M>(zx, S1 + (size_t)M * M, xb, rows, line, t);
+        return;
+      }
+    }
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
       float2 z[EPT];
@@ -1075,8 +1151,9 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   __syncthreads();
   const int wl = blockIdx.y;
   constexpr int NU = p1_units<M, OP>();
+  float2* stash = OP == OP_ADJ ? sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>() : nullptr;
   phase1<M, OP, T, NU>(a, g, w0 + wl, blockIdx.x * NU, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(), sm,
-                       line, t, ahead);
+                       line, t, ahead, stash);
 }
 
 template <int M, int OP>
