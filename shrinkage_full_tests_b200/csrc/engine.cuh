@@ -1323,35 +1323,64 @@ static __global__ void k_wait_selftest(Ctl* ctl, unsigned long long spin_limit) 
 // window (zero outside); adjoint of the central difference
 // (adjointWrtI_kernel, adjoint/srk_adjoint.cuh:25-59).  With ux, uy, v
 // given instead (the reference contract) w = u*v is formed on the fly.
+// A thread computes kStencilCols consecutive columns of one row: the
+// kStencilCols + 2 values of wx it needs are loaded once, and every load is
+// issued before the first use.
+constexpr int kStencilCols = 4;
+template <typename T, bool FROM_U>
+__device__ __forceinline__ void adj_wrt_f_cols(const float* __restrict__ wx, const float* __restrict__ wy,
+                                               const T* __restrict__ v, const T* __restrict__ ux,
+                                               const T* __restrict__ uy, long long wo, long long oo, int N, int W,
+                                               int e, int gx0, int gx1, int gy, T* __restrict__ out) {
+  constexpr int CX = kStencilCols;
+  if (gy >= N) return;
+  const int oy = gy - e;
+  auto w_at = [&](const float* w, const T* u, int r, int c, bool in) -> float {
+    const long long i = wo + (long long)c * W + r;
+    if constexpr (FROM_U) return in ? __fmul_rn(ldf(u, i), ldf(v, i)) : 0.f;
+    else return in ? w[i] : 0.f;
+  };
+  const bool rin = (unsigned)oy < (unsigned)W;
+  const bool uin = (unsigned)(oy - 1) < (unsigned)W, din = (unsigned)(oy + 1) < (unsigned)W;
+  float wxv[CX + 2];
+#pragma unroll
+  for (int j = 0; j < CX + 2; ++j) {
+    const int c = gx0 - e - 1 + j;
+    wxv[j] = w_at(wx, ux, oy, c, rin && (unsigned)c < (unsigned)W);
+  }
+  float wyu[CX], wyd[CX];
+#pragma unroll
+  for (int j = 0; j < CX; ++j) {
+    const int c = gx0 - e + j;
+    const bool cin = (unsigned)c < (unsigned)W;
+    wyu[j] = w_at(wy, uy, oy - 1, c, uin && cin);
+    wyd[j] = w_at(wy, uy, oy + 1, c, din && cin);
+  }
+#pragma unroll
+  for (int j = 0; j < CX; ++j) {
+    const int gx = gx0 + j;
+    if (gx >= gx1) break;
+    const float val = __fadd_rn(__fmul_rn(__fsub_rn(wxv[j], wxv[j + 2]), 0.5f),
+                                __fmul_rn(__fsub_rn(wyu[j], wyd[j]), 0.5f));
+    stf(out, oo + (long long)gx * N + gy, val);
+  }
+}
+
+// Uniform batch: grid (N/32, N/(8*kStencilCols), B) of 32 x 8 blocks.
 template <typename T, bool FROM_U>
 __global__ void k_adj_wrt_f(const float* __restrict__ wx, const float* __restrict__ wy, const T* __restrict__ v,
                             const T* __restrict__ ux, const T* __restrict__ uy, int N, int W, int e, int B,
                             T* __restrict__ out) {
   const int gy = blockIdx.x * blockDim.x + threadIdx.x;
-  const int gx = blockIdx.y * blockDim.y + threadIdx.y;
+  const int gx0 = (blockIdx.y * blockDim.y + threadIdx.y) * kStencilCols;
   const int b = blockIdx.z;
-  if (gx >= N || gy >= N) return;
-  const long long wb = (long long)b * W * W;
-  auto WX = [&](int r, int c) -> float {
-    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
-    const long long i = wb + (long long)c * W + r;
-    if constexpr (FROM_U) return __fmul_rn(ldf(ux, i), ldf(v, i));
-    else return wx[i];
-  };
-  auto WY = [&](int r, int c) -> float {
-    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
-    const long long i = wb + (long long)c * W + r;
-    if constexpr (FROM_U) return __fmul_rn(ldf(uy, i), ldf(v, i));
-    else return wy[i];
-  };
-  const int ox = gx - e, oy = gy - e;
-  const float val = __fadd_rn(__fmul_rn(__fsub_rn(WX(oy, ox - 1), WX(oy, ox + 1)), 0.5f),
-                             __fmul_rn(__fsub_rn(WY(oy - 1, ox), WY(oy + 1, ox)), 0.5f));
-  stf(out, (long long)b * N * N + (long long)gx * N + gy, val);
+  adj_wrt_f_cols<T, FROM_U>(wx, wy, v, ux, uy, (long long)b * W * W, (long long)b * N * N, N, W, e, gx0, N, gy,
+                            out);
 }
 
-// The same for a ragged batch: one 32 x 8 block per block of pixels, the
-// blocks of image b starting at rimg[b].blk0.
+// The same for a ragged batch or a column slab: 32 x 8 blocks over the
+// pixel columns [cx0, cx1) of each image, the blocks of image b starting at
+// rimg[b].blk0.
 template <typename T, bool FROM_U>
 __global__ void k_adj_wrt_f_rag(const float* __restrict__ wx, const float* __restrict__ wy, const T* __restrict__ v,
                                 const T* __restrict__ ux, const T* __restrict__ uy,
@@ -1363,28 +1392,11 @@ __global__ void k_adj_wrt_f_rag(const float* __restrict__ wx, const float* __res
     if (rimg[mid].blk0 <= blk) lo = mid; else hi = mid - 1;
   }
   const RagImage im = rimg[lo];
-  const int N = im.N, W = im.W;
-  const int nby = (N + 31) / 32;
+  const int nby = (im.N + 31) / 32;
   const int k = blk - im.blk0;
   const int gy = (k % nby) * 32 + threadIdx.x;
-  const int gx = im.cx0 + (k / nby) * 8 + threadIdx.y;
-  if (gx >= im.cx1 || gy >= N) return;
-  auto WX = [&](int r, int c) -> float {
-    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
-    const long long i = im.ow + (long long)c * W + r;
-    if constexpr (FROM_U) return __fmul_rn(ldf(ux, i), ldf(v, i));
-    else return wx[i];
-  };
-  auto WY = [&](int r, int c) -> float {
-    if (r < 0 || r >= W || c < 0 || c >= W) return 0.f;
-    const long long i = im.ow + (long long)c * W + r;
-    if constexpr (FROM_U) return __fmul_rn(ldf(uy, i), ldf(v, i));
-    else return wy[i];
-  };
-  const int ox = gx - e, oy = gy - e;
-  const float val = __fadd_rn(__fmul_rn(__fsub_rn(WX(oy, ox - 1), WX(oy, ox + 1)), 0.5f),
-                             __fmul_rn(__fsub_rn(WY(oy - 1, ox), WY(oy + 1, ox)), 0.5f));
-  stf(out, im.on + (long long)gx * N + gy, val);
+  const int gx0 = im.cx0 + ((k / nby) * 8 + threadIdx.y) * kStencilCols;
+  adj_wrt_f_cols<T, FROM_U>(wx, wy, v, ux, uy, im.ow, im.on, im.N, im.W, e, gx0, im.cx1, gy, out);
 }
 
 }  // namespace srk

@@ -116,7 +116,7 @@ template <typename T>
 void adj_wrt_f_t(srk_plan_s* p, const float* wx, const float* wy, const void* v, const void* ux, const void* uy, int B,
                  void* out, cudaStream_t s) {
   const dim3 blk(32, 8);
-  const dim3 grd((p->N + 31) / 32, (p->N + 7) / 8, B);
+  const dim3 grd((p->N + 31) / 32, (p->N + 8 * kStencilCols - 1) / (8 * kStencilCols), B);
   if (ux)
     k_adj_wrt_f<T, true><<<grd, blk, 0, s>>>(nullptr, nullptr, static_cast<const T*>(v), static_cast<const T*>(ux),
                                              static_cast<const T*>(uy), p->N, p->W, p->e, B, static_cast<T*>(out));
@@ -782,7 +782,7 @@ srk_status ragged_tables(srk_plan_s* p, int B, const int* Ns, cudaStream_t s) {
     imgs[b].pad = 0;
     on += (long long)N * N;
     ow += (long long)W * W;
-    blk += (long long)((N + 31) / 32) * ((N + 7) / 8);
+    blk += (long long)((N + 31) / 32) * ((N + 8 * kStencilCols - 1) / (8 * kStencilCols));
     const int Tf = (W + S - 1) / S, Ta = (N + S - 1) / S;
     for (int tx = 0; tx < Tf; ++tx)
       for (int ty = 0; ty < Tf; ++ty) fwd.push_back(make_int4(b, tx * S, ty * S, 0));
@@ -824,7 +824,7 @@ srk_status slab_tables(srk_plan_s* p, int N, int c0, int c1, bool adj, cudaStrea
   imgs[0].cx0 = adj ? c0 : 0;
   imgs[0].cx1 = adj ? c1 : 0;
   imgs[0].pad = 0;
-  const int nblk = adj ? ((N + 31) / 32) * ((c1 - c0 + 7) / 8) : 0;
+  const int nblk = adj ? ((N + 31) / 32) * ((c1 - c0 + 8 * kStencilCols - 1) / (8 * kStencilCols)) : 0;
   std::vector<int4> none;
   return adj ? upload_tables(p, std::move(key), std::move(none), tiles, imgs, nblk, 0, 0, s)
              : upload_tables(p, std::move(key), std::move(tiles), none, imgs, nblk, 0, 0, s);
