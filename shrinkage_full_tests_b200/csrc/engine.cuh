@@ -812,6 +812,40 @@ __device__ __forceinline__ void p1_prefetch(const OpArgs& a, const Geom& g, int 
   asm volatile("prefetch.global.L2 [%0];" ::"l"(img + tr.on + (long long)gx * tr.N + gy));
 }
 
+// The same for the adjoint-type P1 unit xb of WT w2: the v (and dv) columns
+// and the f (and df) columns around them that load_adj_column reads, for
+// both tiles of the pair; one 128-byte line per thread and iteration.
+template <int M, typename T>
+__device__ __forceinline__ void p1_prefetch_adj(const OpArgs& a, const Geom& g, int w2, int xb2) {
+  constexpr int LPU = lpu_of<M>();
+  constexpr int RPL = 128 / (int)sizeof(T);
+  constexpr int LV = (M + RPL - 1) / RPL + 1;      // lines of a v column (start not line-aligned)
+  constexpr int LF = (M + 2 + RPL - 1) / RPL + 1;  // lines of an f column
+  constexpr int PER = LPU * LV + (LPU + 2) * LF;   // per tile and array pair
+  const int npair = a.dI != nullptr ? 2 : 1;
+  const int e = a.e;
+  for (int idx = threadIdx.x; idx < 2 * PER * npair; idx += kThreads) {
+    const int d = idx / (2 * PER), h = (idx / PER) & 1, r = idx % PER;
+    const TileRef tr = tile_of(g, 2 * w2 + h);
+    if (!tr.live) continue;
+    const int x = tr.x0 + xb2 * LPU;
+    if (r < LPU * LV) {
+      const int col = x + r / LV - 2 * e, row0 = tr.y0 - 2 * e;
+      const int row = max(row0, 0) + (r % LV) * RPL;
+      if (col < 0 || col >= tr.W || row >= tr.W || row >= row0 + M) continue;
+      const T* v = static_cast<const T*>(d ? a.dv : a.v);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(v + tr.ow + (long long)col * tr.W + row));
+    } else {
+      const int rf = r - LPU * LV;
+      const int col = x + rf / LF - e - 1, row0 = tr.y0 - e - 1;
+      const int row = max(row0, 0) + (rf % LF) * RPL;
+      if (col < 0 || col >= tr.N || row >= tr.N || row >= row0 + M + 2) continue;
+      const T* f = static_cast<const T*>(d ? a.dI : a.I);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(f + tr.on + (long long)col * tr.N + row));
+    }
+  }
+}
+
 // P1: line `line` transforms column x = xb*LPU + line of every field along
 // y.  NU consecutive units (xb, xb+1, ...) per call, single-field ops only:
 // the next unit's columns are loaded before the current transform, so their
@@ -846,6 +880,10 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
       // both fields from one pass over the inputs; h_y waits in the
       // stash (kThreads x EPT values after the rows, each thread its own)
       if (stash && a.e >= 1) {
+        if (ahead > 0) {
+          const int lin = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
+          p1_prefetch_adj<M, T>(a, g, w - (int)blockIdx.y + lin / (int)gridDim.x, lin % (int)gridDim.x);
+        }
         float2 zx[EPT], zy[EPT];
         load_adj_column<M, T>(a, g, w, xb * LPU + line, t, zx, zy);
         float2* st = stash + threadIdx.x;
