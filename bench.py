@@ -67,18 +67,37 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(N, KW, B):
-    """dram bytes per launch sequence from the committed ncu summary, if any."""
+def profiled_per_image(N, KW, field):
+    """A per-image figure (dram bytes, warp instructions) of the launch
+    sequence from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(path):
         return None
     key = "N=%d KW=%d" % (N, KW)
     with open(path) as fh:
         for line in fh:
-            if line.startswith(key) and "bytes_per_image=" in line:
-                per_img = float(line.split("bytes_per_image=")[1].split()[0])
-                return per_img * B
+            if line.startswith(key) and field + "=" in line:
+                return float(line.split(field + "=")[1].split()[0])
     return None
+
+
+def profiled_traffic(N, KW, B):
+    """dram bytes per launch sequence from the committed ncu summary, if any."""
+    per_img = profiled_per_image(N, KW, "bytes_per_image")
+    return None if per_img is None else per_img * B
+
+
+def issue_bound(N, KW, B, ms, sm_mhz):
+    """The instruction-issue bound of the step: warp instructions (committed
+    ncu count) at one instruction per cycle on each of the 148 x 4 schedulers
+    at the sampled SM clock, against the measured step time."""
+    per_img = profiled_per_image(N, KW, "warp_instructions_per_image")
+    if per_img is None or not sm_mhz:
+        return None
+    rate = 148 * 4 * sm_mhz * 1e6
+    min_ms = per_img * B / rate * 1e3
+    return {"warp_instructions_per_step": per_img * B, "issue_slots_per_s": rate, "min_ms": min_ms,
+            "frac": min_ms / ms, "source": "profiles/traffic.txt (ncu smsp__inst_executed.sum)"}
 
 
 class ClockSampler:
@@ -333,7 +352,8 @@ def run_ours(a):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": "srkTrainingForward launch sequence (P1+P2+P3 per chunk)",
-                         "algorithmic_bytes_per_step": alg_bytes},
+                         "algorithmic_bytes_per_step": alg_bytes,
+                         "issue_bound": issue_bound(N, KW, B, ms, (clocks or {}).get("sm_mhz"))},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
