@@ -68,6 +68,8 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   }
   const size_t smp1 = p1_smem_bytes<M, OP>();
   SRK_TRY(set_smem(k_p1<M, OP, T>, smp1));
+  const bool tan = OP == OP_ADJ && a.dI != nullptr;  // the tangent-adjoint's adjoint-type pass
+  if (tan) SRK_TRY(set_smem(k_p1<M, OP, T, true>, smp1));
   SRK_TRY(set_smem(k_p2<M, OP>, sm2));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
   const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
@@ -90,8 +92,11 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
       s1 = p->side;
       if (w0 > 0) SRK_CUDA(cudaStreamWaitEvent(s1, p->ev_p2, 0));
     }
-    k_p1<M, OP, T><<<dim3(M / LPU / p1_units<M, OP>(), c), kThreads, smp1, s1>>>(a, g, p->tw, w0, p->scratch, g.S,
-                                                                                  p->nsm);
+    const dim3 g1(M / LPU / p1_units<M, OP>(), c);
+    if (tan)
+      k_p1<M, OP, T, true><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, p->scratch, g.S, p->nsm);
+    else
+      k_p1<M, OP, T><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, p->scratch, g.S, p->nsm);
     if (ovl) {
       SRK_CUDA(cudaEventRecord(p->ev_p1, s1));
       SRK_CUDA(cudaStreamWaitEvent(s, p->ev_p1, 0));

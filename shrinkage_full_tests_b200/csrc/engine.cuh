@@ -273,55 +273,64 @@ __device__ __forceinline__ void load_column(const OpArgs& a, const Geom& g, int 
 }
 
 // Both adjoint-type fields of one P1 column at once (erosion >= 1, so every
-// gradient neighbour of the valid window lies inside the image): zx = h_x,
-// zy = h_y of the two tiles of WT w (re / im) at virtual column x, rows
-// lane + TPF i.  Per element one load of v (and dv) and the four neighbours
-// of f (and df), shared by h_x and h_y; the arithmetic is h_at's.
-template <int M, typename T>
+// gradient neighbour of the valid window lies inside the image): zx = h_x of
+// the two tiles of WT w (re / im) at virtual column x, rows lane + TPF i,
+// and h_y of the same element straight into this thread's stash slot
+// st[kThreads i].  Per element one load of v (and dv) and the four
+// neighbours of f (and df), shared by h_x and h_y; the arithmetic is h_at's.
+// TAN: the tangent-adjoint's fields (dv, df given), a compile-time choice so
+// that the plain adjoint carries none of their registers.
+template <int M, typename T, bool TAN>
 __device__ __forceinline__ void load_adj_column(const OpArgs& a, const Geom& g, int w, int x, int lane,
-                                                float2 (&zx)[M / tpf_of<M>()], float2 (&zy)[M / tpf_of<M>()]) {
+                                                float2 (&zx)[M / tpf_of<M>()], float2* __restrict__ st) {
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
-#pragma unroll
-  for (int i = 0; i < EPT; ++i) zx[i] = zy[i] = make_float2(0.f, 0.f);
-  const bool tan = a.dI != nullptr;
+  const T* vc[2];
+  const T* fc[2];
+  const T* dvc[2];
+  const T* dfc[2];
+  int N[2], W[2], oy0[2];
+  bool on[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const TileRef tr = tile_of(g, 2 * w + h);
     const int qx = tr.x0 + x - a.e, ox = qx - a.e;  // image / valid-window column
-    if (!tr.live || ox < 0 || ox >= tr.W) continue;
-    const int qy0 = tr.y0 + lane - a.e, oy0 = qy0 - a.e;
-    const long long vo = tr.ow + (long long)ox * tr.W + oy0;
+    on[h] = tr.live && ox >= 0 && ox < tr.W;
+    const int qy0 = tr.y0 + lane - a.e;
+    oy0[h] = qy0 - a.e;
+    N[h] = tr.N;
+    W[h] = tr.W;
+    const long long vo = tr.ow + (long long)ox * tr.W + oy0[h];
     const long long fo = tr.on + (long long)qx * tr.N + qy0;
-    const T* vc = static_cast<const T*>(a.v) + vo;
-    const T* fc = static_cast<const T*>(a.I) + fo;
-    const T* dvc = tan ? static_cast<const T*>(a.dv) + vo : vc;
-    const T* dfc = tan ? static_cast<const T*>(a.dI) + fo : fc;
-    const int N = tr.N;
+    vc[h] = static_cast<const T*>(a.v) + vo;
+    fc[h] = static_cast<const T*>(a.I) + fo;
+    dvc[h] = TAN ? static_cast<const T*>(a.dv) + vo : vc[h];
+    dfc[h] = TAN ? static_cast<const T*>(a.dI) + fo : fc[h];
+  }
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const bool in = (unsigned)(oy0 + TPF * i) < (unsigned)tr.W;
-      const int o = TPF * i;
-      const float v = in ? ldf(vc, o) : 0.f;
-      const float gx = ((in ? ldf(fc + N, o) : 0.f) - (in ? ldf(fc - N, o) : 0.f)) * 0.5f;
-      const float gy = ((in ? ldf(fc + 1, o) : 0.f) - (in ? ldf(fc - 1, o) : 0.f)) * 0.5f;
-      float hx = v * gx, hy = v * gy;
-      if (tan) {
-        const float dv = in ? ldf(dvc, o) : 0.f;
-        const float dgx = ((in ? ldf(dfc + N, o) : 0.f) - (in ? ldf(dfc - N, o) : 0.f)) * 0.5f;
-        const float dgy = ((in ? ldf(dfc + 1, o) : 0.f) - (in ? ldf(dfc - 1, o) : 0.f)) * 0.5f;
-        hx = dot2(dv, gx, v, dgx);
-        hy = dot2(dv, gy, v, dgy);
+  for (int i = 0; i < EPT; ++i) {
+    const int o = TPF * i;
+    float hx[2], hy[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const bool in = on[h] && (unsigned)(oy0[h] + o) < (unsigned)W[h];
+      const int n = N[h];
+      const float v = in ? ldf(vc[h], o) : 0.f;
+      const float gx = ((in ? ldf(fc[h] + n, o) : 0.f) - (in ? ldf(fc[h] - n, o) : 0.f)) * 0.5f;
+      const float gy = ((in ? ldf(fc[h] + 1, o) : 0.f) - (in ? ldf(fc[h] - 1, o) : 0.f)) * 0.5f;
+      hx[h] = v * gx;
+      hy[h] = v * gy;
+      if constexpr (TAN) {
+        const float dv = in ? ldf(dvc[h], o) : 0.f;
+        const float dgx = ((in ? ldf(dfc[h] + n, o) : 0.f) - (in ? ldf(dfc[h] - n, o) : 0.f)) * 0.5f;
+        const float dgy = ((in ? ldf(dfc[h] + 1, o) : 0.f) - (in ? ldf(dfc[h] - 1, o) : 0.f)) * 0.5f;
+        hx[h] = dot2(dv, gx, v, dgx);
+        hy[h] = dot2(dv, gy, v, dgy);
       }
-      if (!in) hx = hy = 0.f;
-      if (h == 0) {
-        zx[i].x = hx;
-        zy[i].x = hy;
-      } else {
-        zx[i].y = hx;
-        zy[i].y = hy;
-      }
+      if (!in) hx[h] = hy[h] = 0.f;
     }
+    zx[i] = make_float2(hx[0], hx[1]);
+    st[kThreads * i] = make_float2(hy[0], hy[1]);
   }
 }
 
@@ -852,7 +861,7 @@ __device__ __forceinline__ void p1_prefetch_adj(const OpArgs& a, const Geom& g, 
 // latency overlaps it, and the columns of the CTA `ahead` launch positions
 // later (about one per SM: it starts when this one is nearly done) are
 // prefetched into L2.
-template <int M, int OP, typename T, int NU = 1>
+template <int M, int OP, typename T, int NU = 1, bool TAN = false>
 __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, int xb, float2* __restrict__ S1,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
                                        int ahead = 0, float2* __restrict__ stash = nullptr) {
@@ -884,11 +893,9 @@ __device__ __forceinline__ void phase1(const OpArgs& a, const Geom& g, int w, in
           const int lin = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
           p1_prefetch_adj<M, T>(a, g, w - (int)blockIdx.y + lin / (int)gridDim.x, lin % (int)gridDim.x);
         }
-        float2 zx[EPT], zy[EPT];
-        load_adj_column<M, T>(a, g, w, xb * LPU + line, t, zx, zy);
+        float2 zx[EPT];
         float2* st = stash + threadIdx.x;
-#pragma unroll
-        for (int i = 0; i < EPT; ++i) st[kThreads * i] = zy[i];
+        load_adj_column<M, T, TAN>(a, g, w, xb * LPU + line, t, zx, st);
         fft<M, false>(zx, row, tw, t, 1 + line);
         p1_store<M>(zx, S1, xb, rows, line, t);
 #pragma unroll
@@ -1179,9 +1186,11 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
 #endif
 template <int M, int OP>
 __host__ __device__ constexpr int p1_units() { return OpTraits<OP>::K == 1 ? SRK_P1_UNITS : 1; }
-template <int M, int OP, typename T>
+template <int M, int OP, typename T, bool TAN = false>
 __global__ void __launch_bounds__(kThreads, SRK_P1_MIN_BLOCKS)
 k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restrict__ scratch, int S, int ahead) {
+  // TAN (adjoint-type op of the tangent-adjoint, dv and df given) is chosen
+  // by the launch: a.dI != nullptr exactly when TAN
   extern __shared__ float2 sm[];
   constexpr int TPF = tpf_of<M>();
   const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
@@ -1190,8 +1199,8 @@ k_p1(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, float2* __restric
   const int wl = blockIdx.y;
   constexpr int NU = p1_units<M, OP>();
   float2* stash = OP == OP_ADJ ? sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>() : nullptr;
-  phase1<M, OP, T, NU>(a, g, w0 + wl, blockIdx.x * NU, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(), sm,
-                       line, t, ahead, stash);
+  phase1<M, OP, T, NU, TAN>(a, g, w0 + wl, blockIdx.x * NU, scratch + wl * wt_elems<M, OP>(S), sm + tw_slots<M>(),
+                            sm, line, t, ahead, stash);
 }
 
 template <int M, int OP>
