@@ -782,11 +782,10 @@ __device__ __forceinline__ void p1_store(const float2 (&z)[M / tpf_of<M>()], flo
     constexpr int PB = s2_block_pitch<M>();
     constexpr int F4B = LPU * LPU / 2;
     __syncthreads();
+    // ky = t + TPF*i: block t/LPU + i*TPF/LPU, position t % LPU in it
+    float2* rl = rows + (t / LPU) * PB + line * LPU + (t % LPU);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int ky = t + TPF * i;
-      rows[(ky / LPU) * PB + line * LPU + (ky % LPU)] = z[i];
-    }
+    for (int i = 0; i < EPT; ++i) rl[(TPF / LPU) * PB * i] = z[i];
     __syncthreads();
     float2* dst = S1k + (size_t)xb * LPU * LPU;
     for (int j = threadIdx.x; j < (M / LPU) * F4B; j += kThreads) {
@@ -990,10 +989,16 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
       }
       return;
     }
+    {
+      // xv = xb0 + TPF*i lies in block floor(xb0 / LPU) + i*TPF/LPU at
+      // position xb0 mod LPU (an arithmetic shift and a mask also for the
+      // negative xb0 of the columns left of the valid range, never stored)
+      const int xb0 = t - e;
+      constexpr int LS = LPU == 4 ? 2 : 3;
+      float2* tl = tile + (xb0 >> LS) * PB + line * LPU + (xb0 & (LPU - 1));
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) {
-      const int xv = t + TPF * i - e;
-      if (xv >= 0 && xv < S) tile[(xv / LPU) * PB + line * LPU + (xv % LPU)] = o[i];
+      for (int i = 0; i < EPT; ++i)
+        if ((unsigned)(xb0 + TPF * i) < (unsigned)S) tl[(TPF / LPU) * PB * i] = o[i];
     }
     __syncthreads();
     // thread: value pair w of blocks q = q0, q0 + QS, ... (QS blocks per sweep)
@@ -1008,30 +1013,21 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
   row_to_regs<M>(row0, z, t);
   fft<M, false>(z, row0, tw, t, bar);
   if constexpr (K == 1) {
-#ifdef SRK_P2_STASH_REGS
-    float2 zs[EPT];
+    // both spectral products at once; Z*Gy waits in the line's second row
+    // (each thread rereads only its own elements)
+    float2* st = row1 + t + (t >> 4);
 #pragma unroll
-    for (int i = 0; i < EPT; ++i) zs[i] = z[i];
-#pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      const float2* gr = l ? gyr : gxr;
-#pragma unroll
-      for (int i = 0; i < EPT; ++i) z[i] = spec(zs[i], __ldg(gr + TPF * i));
-      fft<M, true>(z, row0, tw, t, bar);
-      emit(z, l);
+    for (int i = 0; i < EPT; ++i) {
+      const float2 zi = z[i];
+      st[RSP * i] = spec(zi, __ldg(gyr + TPF * i));
+      z[i] = spec(zi, __ldg(gxr + TPF * i));
     }
-#else
-    regs_to_row<M>(row1, z, t);  // stash Z(ky, .): each thread rereads only its own elements
+    fft<M, true>(z, row0, tw, t, bar);
+    emit(z, 0);
 #pragma unroll
-    for (int l = 0; l < 2; ++l) {
-      const float2* gr = l ? gyr : gxr;
-      const float2* st = row1 + t + (t >> 4);
-#pragma unroll
-      for (int i = 0; i < EPT; ++i) z[i] = spec(st[RSP * i], __ldg(gr + TPF * i));
-      fft<M, true>(z, row0, tw, t, bar);
-      emit(z, l);
-    }
-#endif
+    for (int i = 0; i < EPT; ++i) z[i] = st[RSP * i];
+    fft<M, true>(z, row0, tw, t, bar);
+    emit(z, 1);
   } else {
     group_sync<TPF>(bar);
     regs_to_row<M>(row0, z, t);  // stash Z0(ky, .) in its own row
