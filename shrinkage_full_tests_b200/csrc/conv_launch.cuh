@@ -103,7 +103,7 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
     }
     k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
     if (ovl) SRK_CUDA(cudaEventRecord(p->ev_p2, s));
-    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0);
+    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0, p->nsm);
     launches += 3;
   }
   p->last_launches = launches;

@@ -1215,7 +1215,7 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
 
 template <int M, int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_P3_MIN_BLOCKS)
-k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0) {
+k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0, int ahead) {
   extern __shared__ float2 sm[];
   constexpr int TPF = tpf_of<M>();
   const int line = threadIdx.x / TPF, t = threadIdx.x % TPF;
@@ -1223,6 +1223,21 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
   const int wl = blockIdx.y;
   constexpr bool ASYNC = p3_async_window<OP, T>();
   T* win0 = ASYNC ? reinterpret_cast<T*>(sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
+  if constexpr (s2_blocked<M>()) {
+    // L2 prefetch of the S2 blocks of the CTA one SM-count of launch
+    // positions later (its LPU columns are one contiguous run per field)
+    constexpr int L = OpTraits<OP>::L;
+    constexpr int LINES = M * lpu_of<M>() * (int)sizeof(float2) / 128;  // per field
+    static_assert(L * LINES <= kThreads, "one line per thread");
+    const int lin = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
+    const int by2 = lin / (int)gridDim.x, bx2 = lin % (int)gridDim.x;
+    if (ahead > 0 && by2 < (int)gridDim.y && threadIdx.x < L * LINES) {
+      const int l = threadIdx.x / LINES, r = threadIdx.x % LINES;
+      const float2* blk = scratch + by2 * wt_elems<M, OP>(g.S) + s1_elems<M, OP>() +
+                          ((size_t)l * (s2_pitch(g.S) / lpu_of<M>()) + bx2) * M * lpu_of<M>();
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(blk + r * (128 / sizeof(float2))));
+    }
+  }
   phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
                           sm + tw_slots<M>(), sm, line, t, win0);
 }
