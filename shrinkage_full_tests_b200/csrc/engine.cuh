@@ -651,9 +651,11 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
         const float2 z0i = z0s[RSP * i];
         const float ux = h ? z0i.y : z0i.x;
         const float uy = h ? z1[i].y : z1[i].x;
-        const float fx = (swin(cp + TPF * i) - swin(cm + TPF * i)) * 0.5f;
-        const float fy = (swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1)) * 0.5f;
-        stf(Rp, TPF * i, dot2(ux, fx, uy, fy));
+        // the central differences' factor 1/2 applied once: halving is
+        // exact, so dot2(ux, dx/2, uy, dy/2) == dot2(ux, dx, uy, dy)/2
+        const float dx = swin(cp + TPF * i) - swin(cm + TPF * i);
+        const float dy = swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1);
+        stf(Rp, TPF * i, dot2(ux, dx, uy, dy) * 0.5f);
       }
       return;
     }
@@ -666,9 +668,9 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
       if (UX) stf(UX, ob + TPF * i, ux);
       if (UY) stf(UY, ob + TPF * i, uy);
       if (R) {
-        const float fx = (swin(cp + TPF * i) - swin(cm + TPF * i)) * 0.5f;
-        const float fy = (swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1)) * 0.5f;
-        stf(R, ob + TPF * i, dot2(ux, fx, uy, fy));
+        const float dx = swin(cp + TPF * i) - swin(cm + TPF * i);
+        const float dy = swin(cc + TPF * i + 1) - swin(cc + TPF * i - 1);
+        stf(R, ob + TPF * i, dot2(ux, dx, uy, dy) * 0.5f);
       }
     }
   } else {
