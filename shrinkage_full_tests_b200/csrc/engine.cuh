@@ -643,13 +643,14 @@ __device__ __forceinline__ void epilogue_staged(const OpArgs& a, const Geom& g, 
     T* __restrict__ UX = static_cast<T*>(a.out_ux);
     T* __restrict__ UY = static_cast<T*>(a.out_uy);
     if (!UX && !UY) {
-      // R only (R is never NULL here): the common case
+      // R only (R is never NULL here): the common case; of the stashed z0
+      // only this round's half is read
       T* __restrict__ Rp = R + ob;
+      const float* z0h = reinterpret_cast<const float*>(z0s) + h;
 #pragma unroll
       for (int i = 0; i < EPT; ++i) {
         if (!(vm >> i & 1u)) continue;
-        const float2 z0i = z0s[RSP * i];
-        const float ux = h ? z0i.y : z0i.x;
+        const float ux = z0h[2 * RSP * i];
         const float uy = h ? z1[i].y : z1[i].x;
         // the central differences' factor 1/2 applied once: halving is
         // exact, so dot2(ux, dx/2, uy, dy/2) == dot2(ux, dx, uy, dy)/2
