@@ -1226,19 +1226,28 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
   const int wl = blockIdx.y;
   constexpr bool ASYNC = p3_async_window<OP, T>();
   T* win0 = ASYNC ? reinterpret_cast<T*>(sm + tw_slots<M>() + 2 * lpu_of<M>() * row_stride<M>()) : nullptr;
-  if constexpr (s2_blocked<M>()) {
-    // L2 prefetch of the S2 blocks of the CTA one SM-count of launch
-    // positions later (its LPU columns are one contiguous run per field)
+  {
+    // L2 prefetch of the S2 columns of the CTA one SM-count of launch
+    // positions later: one contiguous run per field in the blocked layout,
+    // one 8-value row piece per ky in the plain one
     constexpr int L = OpTraits<OP>::L;
-    constexpr int LINES = M * lpu_of<M>() * (int)sizeof(float2) / 128;  // per field
-    static_assert(L * LINES <= kThreads, "one line per thread");
     const int lin = (int)(blockIdx.y * gridDim.x + blockIdx.x) + ahead;
     const int by2 = lin / (int)gridDim.x, bx2 = lin % (int)gridDim.x;
-    if (ahead > 0 && by2 < (int)gridDim.y && threadIdx.x < L * LINES) {
-      const int l = threadIdx.x / LINES, r = threadIdx.x % LINES;
-      const float2* blk = scratch + by2 * wt_elems<M, OP>(g.S) + s1_elems<M, OP>() +
-                          ((size_t)l * (s2_pitch(g.S) / lpu_of<M>()) + bx2) * M * lpu_of<M>();
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(blk + r * (128 / sizeof(float2))));
+    if (ahead > 0 && by2 < (int)gridDim.y) {
+      const float2* s2 = scratch + by2 * wt_elems<M, OP>(g.S) + s1_elems<M, OP>();
+      if constexpr (s2_blocked<M>()) {
+        constexpr int LINES = M * lpu_of<M>() * (int)sizeof(float2) / 128;  // per field
+        static_assert(L * LINES <= kThreads, "one line per thread");
+        if (threadIdx.x < L * LINES) {
+          const int l = threadIdx.x / LINES, r = threadIdx.x % LINES;
+          const float2* blk = s2 + ((size_t)l * (s2_pitch(g.S) / lpu_of<M>()) + bx2) * M * lpu_of<M>();
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(blk + r * (128 / sizeof(float2))));
+        }
+      } else {
+        const float2* col = s2 + bx2 * lpu_of<M>();
+        for (int idx = threadIdx.x; idx < L * M; idx += kThreads)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(col + (size_t)idx * s2_pitch(g.S)));
+      }
     }
   }
   phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
