@@ -53,10 +53,11 @@ typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_
 
 /* Kernel schedule of the convolution engine.  THREE_PASS (default): three
  * launches per chunk of work tiles with the intermediates in a device
- * scratch buffer; with several chunks the first pass of the next chunk runs
- * on a plan-owned side stream next to the last pass of the current one
- * (forked from and joined back into the caller's stream, so the call stays
- * stream-ordered and graph-capturable).  PERSISTENT: one launch per call; the column/row/column
+ * scratch buffer; a call larger than the scratch cycles through a ring of
+ * three scratch slots, the first and last passes on two plan-owned streams
+ * and the middle pass on the caller's, so the passes of neighbouring chunks
+ * run side by side (forked from and joined back into the caller's stream:
+ * the call stays stream-ordered and graph-capturable).  PERSISTENT: one launch per call; the column/row/column
  * passes of every work tile run as tickets of a queue with their
  * intermediates in an L2-resident ring (falls back to THREE_PASS when the
  * scratch holds fewer than three work tiles).  SRK_TILE_AUTOTUNE plans time
@@ -96,9 +97,9 @@ const char* srk_last_error(void);
  * tile_M: 0 = choose by a cost model, SRK_TILE_AUTOTUNE = time every
  *         (tile, schedule) candidate once per device and configuration
  *         (cached on disk, see srk_autotune), else 128, 256 or 512.
- * scratch_budget_bytes: 0 = default (4 GiB, at most 1/32 of the device
- *         memory, at least 256 MiB); the scratch holds a chunk of work tiles
- *         (5.1 MB each at N = 512), never more than B_max needs. */
+ * scratch_budget_bytes: 0 = default (1 GiB); the scratch holds the work
+ *         tiles in flight (5.3 MB each at N = 512), never more than B_max
+ *         needs. */
 srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, int B_max, int spectra_M,
                            srk_dtype dtype, int tile_M, size_t scratch_budget_bytes);
 srk_status srk_plan_destroy(srk_plan plan);

@@ -72,39 +72,57 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   if (tan) SRK_TRY(set_smem(k_p1<M, OP, T, true>, smp1));
   SRK_TRY(set_smem(k_p2<M, OP>, sm2));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
-  const int chunk = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
-  // With several chunks, P1 of chunk k+1 (writes S1) runs on the side
-  // stream next to P3 of chunk k (reads S2): it waits for P2 of chunk k
-  // (the last reader of S1), and P2 of chunk k+1 waits for it and, by the
-  // order of s, for P3 of chunk k (the last reader of S2).  The side stream
-  // is joined back into s by the wait before the last P2.
-  const bool ovl = p->overlap && p->side && nwt > chunk;
-  if (ovl) {
-    SRK_CUDA(cudaEventRecord(p->ev_fork, s));
-    SRK_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
-  }
-  int launches = 0;
-  for (int w0 = 0; w0 < nwt; w0 += chunk) {
-    const int c = (nwt - w0 < chunk) ? (nwt - w0) : chunk;
-    constexpr int LPU = lpu_of<M>();
-    cudaStream_t s1 = s;
-    if (ovl) {
-      s1 = p->side;
-      if (w0 > 0) SRK_CUDA(cudaStreamWaitEvent(s1, p->ev_p2, 0));
-    }
+  constexpr int LPU = lpu_of<M>();
+  auto launch3 = [&](int w0, int c, float2* base, cudaStream_t s1, cudaStream_t s2, cudaStream_t s3,
+                     cudaEvent_t e1, cudaEvent_t e2) -> srk_status {
     const dim3 g1(M / LPU / p1_units<M, OP>(), c);
     if (tan)
-      k_p1<M, OP, T, true><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, p->scratch, g.S, p->nsm);
+      k_p1<M, OP, T, true><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, base, g.S, p->nsm);
     else
-      k_p1<M, OP, T><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, p->scratch, g.S, p->nsm);
-    if (ovl) {
-      SRK_CUDA(cudaEventRecord(p->ev_p1, s1));
-      SRK_CUDA(cudaStreamWaitEvent(s, p->ev_p1, 0));
+      k_p1<M, OP, T><<<g1, kThreads, smp1, s1>>>(a, g, p->tw, w0, base, g.S, p->nsm);
+    if (e1) {
+      SRK_CUDA(cudaEventRecord(e1, s1));
+      SRK_CUDA(cudaStreamWaitEvent(s2, e1, 0));
     }
-    k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s>>>(p->scratch, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
-    if (ovl) SRK_CUDA(cudaEventRecord(p->ev_p2, s));
-    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s>>>(p->scratch, a, g, p->tw, w0, p->nsm);
-    launches += 3;
+    k_p2<M, OP><<<dim3(M / LPU, c), kThreads, sm2, s2>>>(base, p->G[0], p->G[1], conjG ? 1 : 0, g, p->tw);
+    if (e2) {
+      SRK_CUDA(cudaEventRecord(e2, s2));
+      SRK_CUDA(cudaStreamWaitEvent(s3, e2, 0));
+    }
+    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s3>>>(base, a, g, p->tw, w0, p->nsm);
+    return SRK_OK;
+  };
+  const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
+  int launches = 0;
+  constexpr int R = srk_plan_s::kRing;
+  if (nwt <= whole || !p->overlap || !p->ps1 || cap < (size_t)R) {
+    // one chunk at a time on the caller's stream
+    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 3)
+      SRK_TRY(launch3(w0, std::min(whole, nwt - w0), p->scratch, s, s, s, nullptr, nullptr));
+  } else {
+    // A ring of R scratch slots of `chunk` WTs: P1 (own stream) of chunk k
+    // waits for P2 of chunk k-R (the last reader of the slot's S1), P2 (the
+    // caller's stream) for P1 of chunk k and P3 of chunk k-R (the last reader
+    // of its S2), P3 (own stream) for P2 of chunk k.  The phases of up to
+    // three chunks run side by side; both streams fork from and join back
+    // into the caller's stream.
+    const int chunk = (int)std::min<size_t>(cap / R, 65535);
+    const size_t per_slot = (size_t)chunk * per;
+    SRK_CUDA(cudaEventRecord(p->ev_fork, s));
+    SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev_fork, 0));
+    SRK_CUDA(cudaStreamWaitEvent(p->ps3, p->ev_fork, 0));
+    int k = 0;
+    for (int w0 = 0; w0 < nwt; w0 += chunk, ++k, launches += 3) {
+      const int r = k % R;
+      if (k >= R) {
+        SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev2[r], 0));
+        SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[r], 0));
+      }
+      SRK_TRY(launch3(w0, std::min(chunk, nwt - w0), p->scratch + r * per_slot, p->ps1, s, p->ps3, p->ev1[r],
+                      p->ev2[r]));
+      SRK_CUDA(cudaEventRecord(p->ev3[r], p->ps3));
+    }
+    SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[(k - 1) % R], 0));  // joins P3; P1 joined through P2
   }
   p->last_launches = launches;
   return cuda_status(cudaGetLastError(), "conv launch");

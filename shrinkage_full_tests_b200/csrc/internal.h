@@ -54,6 +54,9 @@ inline srk_status cuda_status(cudaError_t e, const char* what) {
 
 }  // namespace srk
 
+#ifndef SRK_RING
+#define SRK_RING 3
+#endif
 struct srk_plan_s {
   int device = 0;
   int nsm = 0;  // SMs of the device (P1's L2 prefetch distance)
@@ -81,10 +84,13 @@ struct srk_plan_s {
   unsigned long long* mailbox_spins = nullptr;  // pinned: spin polls of the last launch
   int persist_lag = 0, persist_grid = 0, persist_prefetch = 0;
   int last_grid = 0, last_launches = 0, last_lag = 0, last_nslot = 0;
-  // three-pass schedule: P1 of chunk k+1 runs on a side stream while P3 of
-  // chunk k finishes (S1 and S2 are separate regions of the scratch)
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_p1 = nullptr, ev_p2 = nullptr;
+  // three-pass schedule over several chunks: a ring of kRing scratch slots,
+  // P1 / P3 on streams of their own and P2 on the caller's, ordered per slot
+  // by events, so the three phases of different chunks run side by side
+  static constexpr int kRing = SRK_RING;
+  cudaStream_t ps1 = nullptr, ps3 = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev1[kRing] = {}, ev2[kRing] = {}, ev3[kRing] = {};
   bool overlap = true;
   // ragged batches: device tables of the last ragged call (tile -> image,
   // per-image sizes/offsets), rebuilt only when the image sizes change

@@ -379,15 +379,10 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
                                            (size_t)B_max * p->T * p->T,
                                            (size_t)(B_max * (size_t)p->Ta * p->Ta + 1) / 2});
   const size_t per = wt_bytes(M, p->S);
-  // default scratch: 4 GiB, at most 1/32 of the device memory, at least 256 MiB
-  // (larger chunks mean fewer launch boundaries: 1 -> 4 GiB is -2% at B=5000,
-  // N=512 on the B200)
-  size_t cap = budget;
-  if (!cap) {
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    cap = std::max<size_t>((size_t)256 << 20, std::min<size_t>((size_t)4 << 30, total_b / 32));
-  }
+  // default scratch: 1 GiB (the three-pass ring of chunks runs the phases of
+  // neighbouring chunks side by side, so a larger scratch buys almost
+  // nothing: within 0.5% from 1 to 8 GiB at B=5000, N=512 on the B200)
+  const size_t cap = budget ? budget : ((size_t)1 << 30);
   size_t chunk = cap / per;
   if (chunk < 1) chunk = 1;
   if (chunk > nwt_max) chunk = nwt_max;
@@ -416,11 +411,15 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   *p->mailbox_spins = 0;
   if ((err = cudaEventCreateWithFlags(&p->mailbox_ev, cudaEventDisableTiming)) != cudaSuccess)
     return cleanup(cuda_status(err, "event creation"));
-  if ((err = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking)) != cudaSuccess)
-    return cleanup(cuda_status(err, "stream creation"));
-  for (cudaEvent_t* ev : {&p->ev_fork, &p->ev_p1, &p->ev_p2})
-    if ((err = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
-      return cleanup(cuda_status(err, "event creation"));
+  for (cudaStream_t* st : {&p->ps1, &p->ps3})
+    if ((err = cudaStreamCreateWithFlags(st, cudaStreamNonBlocking)) != cudaSuccess)
+      return cleanup(cuda_status(err, "stream creation"));
+  if ((err = cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming)) != cudaSuccess)
+    return cleanup(cuda_status(err, "event creation"));
+  for (int r = 0; r < srk_plan_s::kRing; ++r)
+    for (cudaEvent_t* ev : {&p->ev1[r], &p->ev2[r], &p->ev3[r]})
+      if ((err = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
+        return cleanup(cuda_status(err, "event creation"));
   // per-pass twiddle blocks (tw_entry), exp(-2 pi i num/den) in double, rounded once
   std::vector<float2> tw(M, make_float2(0.f, 0.f));
   for (int m = 0; m < tw_entries(M); ++m) {
@@ -450,9 +449,12 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->mailbox) cudaFreeHost(p->mailbox);
   if (p->mailbox_spins) cudaFreeHost(p->mailbox_spins);
   if (p->mailbox_ev) cudaEventDestroy(p->mailbox_ev);
-  for (cudaEvent_t ev : {p->ev_fork, p->ev_p1, p->ev_p2})
-    if (ev) cudaEventDestroy(ev);
-  if (p->side) cudaStreamDestroy(p->side);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  for (int r = 0; r < srk_plan_s::kRing; ++r)
+    for (cudaEvent_t ev : {p->ev1[r], p->ev2[r], p->ev3[r]})
+      if (ev) cudaEventDestroy(ev);
+  for (cudaStream_t st : {p->ps1, p->ps3})
+    if (st) cudaStreamDestroy(st);
   delete p;
   return SRK_OK;
 }

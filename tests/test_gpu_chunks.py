@@ -1,8 +1,9 @@
 """Work tiles in several scratch chunks.  A small scratch budget splits a
-batch into chunks whose first pass (P1) runs on the plan's side stream next
-to the previous chunk's last pass (P3).  Results must be bit-identical to a
-single-chunk plan (the work tiles and their pairing do not depend on the
-chunking), directly and replayed from a CUDA graph."""
+batch into chunks that cycle through a ring of scratch slots, P1 and P3 on
+the plan's own streams and P2 on the caller's, so the passes of neighbouring
+chunks overlap.  Results must be bit-identical to a single-chunk plan (the
+work tiles and their pairing do not depend on the chunking), directly and
+replayed from a CUDA graph."""
 import numpy as np
 import pytest
 
@@ -25,16 +26,16 @@ def test_chunked_training_forward_bit_identical_and_capturable(torch_cuda):
     one.set_schedule(srk.SRK_SCHEDULE_THREE_PASS)
     assert one.info()["chunk_wt"] >= B // 2
     per_wt = one.info()["scratch_bytes"] // one.info()["chunk_wt"]
-    many = srk.SrkPlan(N, W, e, 1.0, B, tile_M=256, scratch_budget=3 * per_wt)
+    many = srk.SrkPlan(N, W, e, 1.0, B, tile_M=256, scratch_budget=6 * per_wt)
     many.set_schedule(srk.SRK_SCHEDULE_THREE_PASS)
-    assert many.info()["chunk_wt"] == 3
+    assert many.info()["chunk_wt"] == 6  # a ring of three slots of two work tiles
     E = dev(np.stack(fields(N, B, 70)), torch)
     R1 = torch.zeros((B, W, W), device="cuda")
     R2 = torch.zeros((B, W, W), device="cuda")
     srk.srkTrainingForward(E, E, GX, GY, N, W, e, 1.0, B, None, R1, one)
     srk.srkTrainingForward(E, E, GX, GY, N, W, e, 1.0, B, None, R2, many)
     torch.cuda.synchronize()
-    assert many.info()["last_launches"] == 3 * 4  # 11 work tiles in chunks of 3
+    assert many.info()["last_launches"] == 3 * 6  # 11 work tiles in chunks of 2
     assert torch.equal(R1, R2)
     # captured: the side stream forks from and joins the capturing stream
     stream = torch.cuda.Stream()

@@ -1,7 +1,7 @@
 """The training forward at the benchmark's full size: B = 5000 images of
 N = 512, KW = 121 (W = 392), dx = 4 nm, Green's tensor of gamma = 1/30 nm,
 Gaussian random fields generated on the device; the default plan splits the
-batch into several scratch chunks (side-stream overlap included).
+batch into several scratch chunks (through the ring of scratch slots).
 
 * every image against the reference's own cuFFT srkTrainingForward compiled
   from its sources (when built), to the reference forward tolerance;
