@@ -97,9 +97,9 @@ const char* srk_last_error(void);
  * tile_M: 0 = choose by a cost model, SRK_TILE_AUTOTUNE = time every
  *         (tile, schedule) candidate once per device and configuration
  *         (cached on disk, see srk_autotune), else 128, 256 or 512.
- * scratch_budget_bytes: 0 = default (1 GiB); the scratch holds the work
- *         tiles in flight (5.3 MB each at N = 512), never more than B_max
- *         needs. */
+ * scratch_budget_bytes: 0 = default (8 GiB, at most 1/16 of the device
+ *         memory, at least 256 MiB); the scratch holds the work tiles in
+ *         flight (5.8 MB each at N = 512), never more than B_max needs. */
 srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, int B_max, int spectra_M,
                            srk_dtype dtype, int tile_M, size_t scratch_budget_bytes);
 srk_status srk_plan_destroy(srk_plan plan);
