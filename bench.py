@@ -501,10 +501,26 @@ def run_reference(a):
                                    "cpu_conv_valid, adjoint/main_adjoint.cu:70-90)" % sample},
         "e2e": {"value": rate, "unit": "img/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line["cpu_reference_f32_1thread"] = cpu_checker_f32_rate(N, KW, dx, Kx, Ky, imgs[0].astype(np.float32))
     line["gpu_reference"] = gpu_reference(a)
     line["gpu_reference_oas"] = gpu_reference_oas()
     line["gpu_reference_cudnn"] = gpu_reference_cudnn(a)
     print(json.dumps(line))
+
+
+def cpu_checker_f32_rate(N, KW, dx, Kx, Ky, img, cols=16):
+    """The reference's own CPU checker form (cpu_conv_valid + combine,
+    adjoint/main_adjoint.cu:70-90, :321-333: float, one thread) timed on
+    `cols` output columns of one image and scaled to whole images."""
+    from oracle import oracle as O
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    t0 = time.perf_counter()
+    O.forward_f32_cols(img, img, Kx, Ky, e, dx, W // 2, cols)
+    el = time.perf_counter() - t0
+    return {"value": cols / W / el, "unit": "img/s", "cores": 1, "kind": "port",
+            "sample": "%d of %d output columns of one N=%d KW=%d image (%.2f s), scaled to a whole image"
+                      % (cols, W, N, KW, el)}
 
 
 def gpu_reference_oas(N=4096, KW=61, M=1024, reps=5):

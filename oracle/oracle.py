@@ -49,6 +49,7 @@ def lib():
         L.oracle_make_kernel.argtypes = [i, ctypes.c_float, ctypes.c_float, ctypes.c_float, _fp, _fp]
         L.oracle_kernel_freq.argtypes = [_fp, i, i, _fp]
         L.oracle_grad.argtypes = [_dp, i, _dp, _dp]
+        L.oracle_forward_f32_cols.argtypes = [_fp, _fp, i, _fp, _fp, i, i, ctypes.c_float, i, i, _fp]
         _lib = L
     return _lib
 
@@ -104,6 +105,22 @@ def forward(E, I, Gx, Gy, erosion, dx, window=None, nthreads=None, return_u=Fals
     lib().oracle_forward_window(pE, pI, N, pGx, pGy, KW, erosion, dx, ox0, oy0, wx, wy, R.ctypes.data_as(_dp),
                                 ux.ctypes.data_as(_dp), uy.ctypes.data_as(_dp), nthreads or nthreads_default())
     return (R, ux, uy) if return_u else R
+
+
+def forward_f32_cols(E, I, Gx, Gy, erosion, dx, ox0, wx):
+    """Output columns [ox0, ox0+wx) of the forward in the reference CPU
+    checker's own form (single-thread float, cpu_conv_valid's loop order):
+    the timing row of the measurement, not the checker."""
+    E = np.ascontiguousarray(E, np.float32)
+    I = np.ascontiguousarray(I, np.float32)
+    Gx = np.ascontiguousarray(Gx, np.float32)
+    Gy = np.ascontiguousarray(Gy, np.float32)
+    N, KW = E.shape[0], Gx.shape[0]
+    W = N - 2 * erosion
+    R = np.empty((wx, W), np.float32)
+    lib().oracle_forward_f32_cols(E.ctypes.data_as(_fp), I.ctypes.data_as(_fp), N, Gx.ctypes.data_as(_fp),
+                                  Gy.ctypes.data_as(_fp), KW, erosion, dx, ox0, wx, R.ctypes.data_as(_fp))
+    return R
 
 
 def adj_wrt_I(v, ux, uy, N, erosion):

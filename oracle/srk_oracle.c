@@ -141,6 +141,42 @@ void oracle_forward_window(const double* E, const double* I, int N, const double
   if (!uy_out) free(uy);
 }
 
+/* ---- the reference's own CPU checker form, for timing ----------------------
+ * cpu_conv_valid (adjoint/main_adjoint.cu:70-90) is a single-thread float
+ * loop: output rows outer, columns inner, kernel rows outer, kernel columns
+ * inner, zero outside the image.  This restates it (two kernels, then the
+ * combine of :321-333 with the gradient rule) on the output columns
+ * [ox0, ox0+wx), so that the measurement can time a bounded sample of an
+ * image with the reference's arithmetic type and loop order.  The FP64
+ * functions above are the checker.  R[(ox-ox0)*W + oy]. */
+static float conv_f32_at(const float* E, int N, const float* G, int KW, int gx, int gy) {
+  const int c = KW / 2;
+  float sum = 0.f;
+  for (int ky = -c; ky <= c; ++ky)
+    for (int kx = -c; kx <= c; ++kx) {
+      const int y = gy - ky, x = gx - kx;
+      if (y >= 0 && y < N && x >= 0 && x < N) sum += E[(long long)x * N + y] * G[(kx + c) * KW + (ky + c)];
+    }
+  return sum;
+}
+
+void oracle_forward_f32_cols(const float* E, const float* I, int N, const float* Gx, const float* Gy, int KW, int e,
+                             float dx, int ox0, int wx, float* R) {
+  const int W = N - 2 * e;
+  const float scale = dx * dx;
+  for (int oy = 0; oy < W; ++oy)
+    for (int ox = ox0; ox < ox0 + wx; ++ox) {
+      const int gx = ox + e, gy = oy + e;
+      const float ux = scale * conv_f32_at(E, N, Gx, KW, gx, gy);
+      const float uy = scale * conv_f32_at(E, N, Gy, KW, gx, gy);
+      const float r = (gx < N - 1) ? I[(long long)(gx + 1) * N + gy] : 0.f;
+      const float l = (gx > 0) ? I[(long long)(gx - 1) * N + gy] : 0.f;
+      const float d = (gy < N - 1) ? I[(long long)gx * N + gy + 1] : 0.f;
+      const float u = (gy > 0) ? I[(long long)gx * N + gy - 1] : 0.f;
+      R[(long long)(ox - ox0) * W + oy] = ux * ((r - l) * 0.5f) + uy * ((d - u) * 0.5f);
+    }
+}
+
 void oracle_forward(const double* E, const double* I, int N, const double* Gx, const double* Gy, int KW, int W,
                     int e, double dx, double* R, double* ux, double* uy, int nthreads) {
   oracle_forward_window(E, I, N, Gx, Gy, KW, e, dx, 0, 0, W, W, R, ux, uy, nthreads);

@@ -154,3 +154,16 @@ def test_grf_filter_reproduces_reference_generator(N, ell, seed):
     ref = O.ref_gp_field(N, ell, seed).astype(np.float64)
     ours = O.grf_filter(O.ref_gp_noise(N, seed), N, ell)
     assert np.abs(ours - ref).max() < 1e-6 * np.abs(ref).max()
+
+
+def test_reference_checker_form_matches_oracle():
+    """The single-thread float restatement of cpu_conv_valid + combine (the
+    timing row of the reference arm) agrees with the FP64 oracle."""
+    N, KW = 64, 15
+    e = (KW - 1) // 2
+    Kx, Ky = O.make_kernel_sigma(KW, e / 3.0)
+    f = O.grf(N, 8.0, 77)
+    R64 = O.forward(f, f, Kx, Ky, e, 1.0)
+    R32 = O.forward_f32_cols(f, f, Kx, Ky, e, 1.0, 3, 9)
+    ref = R64[3:12]
+    assert np.abs(R32 - ref).max() < 1e-4 * np.abs(R64).max()
