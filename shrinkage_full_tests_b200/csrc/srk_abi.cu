@@ -304,8 +304,14 @@ bool tune_lookup(const std::string& key, int* M, int* sched) {
   char k[256];
   int m = 0, sc = 0;
   bool found = false;
+  // entries are appended one line per write (ranks of one node may share
+  // the file); anything that is not a valid (tile, schedule) pair is ignored
   while (fscanf(f, "%255s %d %d", k, &m, &sc) == 3)
-    if (key == k) { *M = m; *sched = sc; found = true; }
+    if (key == k && (m == 128 || m == 256 || m == 512) && (sc == 0 || sc == 1)) {
+      *M = m;
+      *sched = sc;
+      found = true;
+    }
   fclose(f);
   return found;
 }
