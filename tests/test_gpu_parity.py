@@ -343,6 +343,16 @@ def test_half_storage_derivatives(torch_cuda, dtype):
     of, og = O.tangent_adjoint(fh, gh, dfh, dgh, lamh, dlamh, Kx, Ky, e, 1.0, "reference")
     assert rel_max_err(back(dlf), of) < 1e-2
     assert rel_max_err(back(dlg), og) < 1e-2
+    # the adjoint (reference contract: v, ux, uy given) in the same storage
+    _, uxo, uyo = O.forward(gh, fh, Kx, Ky, e, 1.0, return_u=True)
+    UX, UY = hp(uxo.astype(np.float32)), hp(uyo.astype(np.float32))
+    dI = torch.zeros((N, N), device="cuda", dtype=tdt)
+    dE = torch.zeros((N, N), device="cuda", dtype=tdt)
+    srk.adjointSRK(LAM, UX, UY, F, GX, GY, N, W, e, 1.0, None, dI, dE, plan)
+    plan.sync()
+    uxh, uyh = back(UX), back(UY)
+    assert rel_max_err(back(dI), O.adj_wrt_I(lamh, uxh, uyh, N, e)) < 1e-2
+    assert rel_max_err(back(dE), O.adj_wrt_E(lamh, fh, Kx, Ky, e, 1.0, "reference")) < 1e-2
 
 
 def test_autotuned_plan_is_correct_and_cached(torch_cuda, tmp_path, monkeypatch):
