@@ -219,7 +219,7 @@ def max_over_ranks(torch, dist, x):
     return float(v.item())
 
 
-def e2e_pipeline(torch, srk, plan, GX, GY, N, W, e, dx, B, steps, warmup, dist, chunk=125):
+def e2e_pipeline(torch, srk, plan, GX, GY, N, W, e, dx, B, steps, warmup, dist, chunk=32):
     """Host-buffer end to end: pinned host E -> device, forward, device -> pinned
     host R, chunked over three streams so copies overlap compute."""
     Eh = torch.empty((B, N, N), dtype=torch.float32).pin_memory()
@@ -311,7 +311,7 @@ def run_ours(a):
                                         1, dist)
         ms_e2e = max_over_ranks(torch, dist, ms_e2e)
         e2e = {"value": world * B / (ms_e2e * 1e-3), "unit": "img/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e, "pipeline": "3 streams, 125-image chunks"}
+               "d2h_bytes_per_step": d2h, "ms_per_step": ms_e2e, "pipeline": "3 streams, 32-image chunks"}
 
     ops = None
     if not a.no_ops and world == 1:
