@@ -57,8 +57,9 @@ typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_
  * three scratch slots, the first and last passes on two plan-owned streams
  * and the middle pass on the caller's, so the passes of neighbouring chunks
  * run side by side (forked from and joined back into the caller's stream:
- * the call stays stream-ordered and graph-capturable).  PERSISTENT: one launch per call; the column/row/column
- * passes of every work tile run as tickets of a queue with their
+ * the call stays stream-ordered and graph-capturable).  PERSISTENT: one
+ * launch per call; the column/row/column passes of every work tile run as
+ * tickets of a queue with their
  * intermediates in an L2-resident ring (falls back to THREE_PASS when the
  * scratch holds fewer than three work tiles).  SRK_TILE_AUTOTUNE plans time
  * both and keep the faster. */
@@ -228,12 +229,20 @@ srk_status srk_tangent_adjoint_ragged(const float* d_f, const float* d_g, const 
  *   forward, tangent: N-sized inputs columns [c0, c1 + 2*erosion); R / dh [c0, c1).
  *   adjoint: v, ux, uy (W-sized) columns [c0 - 2*erosion, c1); I columns
  *            [c0 - erosion - 1, c1 + erosion + 1); dLdI, dLdE [c0, c1).
+ *   tangent-adjoint (outputs: columns [c0, c1) of dLam_f, dLam_g): f, df
+ *            [c0 - erosion - 1, c1 + erosion + 1); g, dg [r0, rE + 2*erosion);
+ *            lam, dlam [min(c0 - 2*erosion, r0), max(c1, rE)), where
+ *            r0 = max(c0 - erosion - 1, 0), r1 = min(c1 - erosion + 1, W),
+ *            rE = min(r0 + T*S, W) with T = ceil((r1 - r0) / S) whole tiles
+ *            of the plan's tile_stride S (the W-sized intermediate of the
+ *            dL/df part is computed by whole tiles from r0).
  * c1 - c0 must be a multiple of the plan's tile_stride (srk_plan_get_info)
- * unless c1 is the last output column (W, or N for the adjoint).  The plan
- * is one made for the whole image (N <= its N).  The reference has no slab
- * form; these replace srkForwardOaS (srk_forward.cuh:468-501),
- * shrinkageTangentOaS (srk_tangent.cuh:111-151) and adjointSRK
- * (srk_adjoint.cuh:402-425) on one slab. */
+ * unless c1 is the last output column (W, or N for the adjoint-type
+ * outputs).  The plan is one made for the whole image (N <= its N).  The
+ * reference has no slab form; these replace srkForwardOaS
+ * (srk_forward.cuh:468-501), shrinkageTangentOaS (srk_tangent.cuh:111-151),
+ * adjointSRK (srk_adjoint.cuh:402-425) and shrinkageTangentAdjointOaS
+ * (srk_tangent_adjoint.cuh:105-159) on one slab. */
 srk_status srk_forward_oas_slab(const float* d_E, const float* d_I, const void* d_Gx_freq,
                                 const void* d_Gy_freq, int N, int erosion, float dx, int c0, int c1,
                                 srk_stream_t stream, float* d_R, srk_plan plan);
@@ -244,6 +253,10 @@ srk_status srk_adjoint_slab(const float* d_v, const float* d_ux, const float* d_
                             const void* d_Gx_freq, const void* d_Gy_freq, int N, int erosion, float dx,
                             int c0, int c1, srk_stream_t stream, float* d_dLdI, float* d_dLdE,
                             srk_plan plan);
+srk_status srk_tangent_adjoint_slab(const float* d_f, const float* d_g, const float* d_df, const float* d_dg,
+                                    const float* d_lam_h, const float* d_dlam_h, const void* d_Gx_freq,
+                                    const void* d_Gy_freq, int N, int erosion, float dx, int c0, int c1,
+                                    srk_stream_t stream, float* d_dLam_f, float* d_dLam_g, srk_plan plan);
 
 /* ---- synthetic inputs on the device -----------------------------------------
  * Gaussian random fields as GpGenerator (third_party/include/stTestCore/

@@ -97,6 +97,7 @@ _SIGS = {
     "srk_forward_oas_slab": [_P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P],
     "srk_tangent_slab": [_P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P],
     "srk_adjoint_slab": [_P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P, _P],
+    "srk_tangent_adjoint_slab": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _F, _I, _I, _P, _P, _P, _P],
 }
 # storage-typed forms (void* buffers in the plan's dtype): same argument types
 for _n in ("srk_training_forward", "srk_forward_oas", "srk_adjoint", "srk_tangent", "srk_tangent_adjoint",
@@ -295,6 +296,13 @@ def shrinkageTangentOaSSlab(f, g, df, dg, Gx_freq, Gy_freq, N, erosion, dx, c0, 
 def adjointSRKSlab(v, ux, uy, I, Gx_freq, Gy_freq, N, erosion, dx, c0, c1, stream, dLdI, dLdE, ws):
     _check(lib().srk_adjoint_slab(_ptr(v), _ptr(ux), _ptr(uy), _ptr(I), _ptr(Gx_freq), _ptr(Gy_freq), N, erosion,
                                   dx, c0, c1, _stream(stream), _ptr(dLdI), _ptr(dLdE), ws.handle))
+
+
+def shrinkageTangentAdjointOaSSlab(f, g, df, dg, lam_h, dlam_h, Gx_freq, Gy_freq, N, erosion, dx, c0, c1, stream,
+                                   dLam_f, dLam_g, ws):
+    _check(lib().srk_tangent_adjoint_slab(_ptr(f), _ptr(g), _ptr(df), _ptr(dg), _ptr(lam_h), _ptr(dlam_h),
+                                          _ptr(Gx_freq), _ptr(Gy_freq), N, erosion, dx, c0, c1, _stream(stream),
+                                          _ptr(dLam_f), _ptr(dLam_g), ws.handle))
 
 
 # ---- synthetic inputs on the device

@@ -844,6 +844,44 @@ srk_status slab_tables(srk_plan_s* p, int N, int c0, int c1, bool adj, cudaStrea
              : upload_tables(p, std::move(key), std::move(tiles), none, imgs, nblk, 0, 0, s);
 }
 
+// The tangent-adjoint on the slab [c0, c1) of the N x N outputs: adjoint-type
+// tiles over [c0, c1), and forward-type tiles over the W-columns of its
+// intermediate (wx, wy) that the dL/df stencil reads, [c0-e-1, c1-e+1)
+// clipped to [0, W): whole tiles from r0 = max(c0-e-1, 0), so the forward-type
+// part covers [r0, rE) with rE - r0 a multiple of S (or rE = W).  One image;
+// the pointers address column c0 of every array.
+srk_status slab_tables_ta(srk_plan_s* p, int N, int c0, int c1, int* r0o, int* rEo, cudaStream_t s) {
+  const int e = p->e, S = p->S, W = N - 2 * e;
+  if (N < 2 * e + 1 || N > p->N)
+    return fail(SRK_ERR_INVALID_ARG, "slab image N=%d outside [2*erosion+1=%d, plan N=%d]", N, 2 * e + 1, p->N);
+  if (c0 < 0 || c1 <= c0 || c1 > N) return fail(SRK_ERR_INVALID_ARG, "slab columns [%d, %d) outside [0, %d)", c0, c1, N);
+  if ((c1 - c0) % S != 0 && c1 != N)
+    return fail(SRK_ERR_INVALID_ARG, "slab [%d, %d) must span whole tiles of %d columns or end at column %d", c0, c1,
+                S, N);
+  const int r0 = std::max(c0 - e - 1, 0), r1 = std::min(c1 - e + 1, W);
+  const int T = r1 > r0 ? (r1 - r0 + S - 1) / S : 0;
+  *r0o = r0;
+  *rEo = T ? std::min(r0 + T * S, W) : r0;
+  std::vector<int> key = {-3, N, c0, c1};
+  if (key == p->rag_key) return SRK_OK;
+  std::vector<int4> fwd, adj;
+  for (int k = 0; k < T; ++k)
+    for (int y0 = 0; y0 < W; y0 += S) fwd.push_back(make_int4(0, r0 + k * S, y0, 0));
+  for (int x0 = c0; x0 < c1; x0 += S)
+    for (int y0 = 0; y0 < N; y0 += S) adj.push_back(make_int4(0, x0, y0, 0));
+  std::vector<RagImage> imgs(1);
+  imgs[0].on = -(long long)c0 * N;
+  imgs[0].ow = -(long long)c0 * W;
+  imgs[0].N = N;
+  imgs[0].W = W;
+  imgs[0].blk0 = 0;
+  imgs[0].cx0 = c0;
+  imgs[0].cx1 = c1;
+  imgs[0].pad = 0;
+  const int nblk = ((N + 31) / 32) * ((c1 - c0 + 8 * kStencilCols - 1) / (8 * kStencilCols));
+  return upload_tables(p, std::move(key), std::move(fwd), adj, imgs, nblk, 0, 0, s);
+}
+
 Geom ragged_geom(const srk_plan_s* p, bool adj) {
   Geom g = adj ? adj_geom(p, 1) : fwd_geom(p, 1);
   g.U = adj ? p->rag_ntiles_adj : p->rag_ntiles_fwd;
@@ -1016,6 +1054,38 @@ srk_status op_adjoint_slab(const void* v, const void* ux, const void* uy, const 
   return launch_conv_dt<OP_ADJ>(p, a, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
 }
 
+srk_status op_tangent_adjoint_slab(const void* f, const void* g, const void* df, const void* dg, const void* lam,
+                                   const void* dlam, const void* gx, const void* gy, int N, int erosion, float dx,
+                                   int c0, int c1, srk_stream_t s, void* dLam_f, void* dLam_g, srk_plan p) {
+  const NvtxRange nvtx_range("srk_tangent_adjoint_slab");
+  SRK_TRY(check_ragged(p, erosion, dx));
+  SRK_NONNULL(f);
+  SRK_NONNULL(g);
+  SRK_NONNULL(df);
+  SRK_NONNULL(dg);
+  SRK_NONNULL(lam);
+  SRK_NONNULL(dlam);
+  SRK_NONNULL(dLam_f);
+  SRK_NONNULL(dLam_g);
+  SRK_TRY(enter(p, s));
+  SRK_TRY(bind_spectra(p, gx, gy, s));
+  int r0 = 0, rE = 0;
+  SRK_TRY(slab_tables_ta(p, N, c0, c1, &r0, &rE, s));
+  const int W = N - 2 * p->e;
+  const size_t ww = (size_t)(rE - r0) * W;
+  SRK_TRY(ensure_wbuf(p, std::max<size_t>(2 * ww, 1) * sizeof(float), s));
+  // wx, wy hold the W-columns [r0, rE); their pointers address column c0
+  float* wx = p->wbuf + (ptrdiff_t)(c0 - r0) * W;
+  float* wy = wx + ww;
+  OpArgs a = base_args(p);
+  a.E = g; a.dE = dg; a.v = lam; a.dv = dlam; a.out0 = wx; a.out1 = wy;
+  SRK_TRY(launch_conv_dt<OP_TANADJ_F>(p, a, ragged_geom(p, false), false, s));
+  SRK_TRY(adj_wrt_f_rag(p, wx, wy, nullptr, nullptr, nullptr, 1, dLam_f, s));
+  OpArgs b = base_args(p);
+  b.v = lam; b.dv = dlam; b.I = f; b.dI = df; b.out0 = dLam_g;
+  return launch_conv_dt<OP_ADJ>(p, b, ragged_geom(p, true), p->conv == SRK_ADJ_TRUE, s);
+}
+
 // The float* entry points are the reference drop-ins: fp32 plans only.
 srk_status need_f32(srk_plan p) {
   if (p && p->dtype != SRK_F32)
@@ -1100,6 +1170,14 @@ srk_status srk_adjoint_slab(const float* v, const float* ux, const float* uy, co
                             float* dLdI, float* dLdE, srk_plan p) {
   SRK_TRY(need_f32(p));
   return op_adjoint_slab(v, ux, uy, I, gx, gy, N, erosion, dx, c0, c1, s, dLdI, dLdE, p);
+}
+
+srk_status srk_tangent_adjoint_slab(const float* f, const float* g, const float* df, const float* dg,
+                                    const float* lam, const float* dlam, const void* gx, const void* gy, int N,
+                                    int erosion, float dx, int c0, int c1, srk_stream_t s, float* dLam_f,
+                                    float* dLam_g, srk_plan p) {
+  SRK_TRY(need_f32(p));
+  return op_tangent_adjoint_slab(f, g, df, dg, lam, dlam, gx, gy, N, erosion, dx, c0, c1, s, dLam_f, dLam_g, p);
 }
 
 srk_status srk_forward_oas_ragged(const float* E, const float* I, const void* gx, const void* gy, int B,

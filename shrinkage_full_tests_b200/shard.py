@@ -146,8 +146,54 @@ def adjoint_slabs(v, ux, uy, I, N, erosion, stride, rank, world, dist, op):
     return dLdI, dLdE
 
 
+def ta_wrange(lo, hi, N, erosion, stride):
+    """W-columns [r0, rE) of the tangent-adjoint's intermediate that its slab
+    [lo, hi) computes by whole tiles (srk_tangent_adjoint_slab)."""
+    e = erosion
+    W = N - 2 * e
+    r0, r1 = max(lo - e - 1, 0), min(hi - e + 1, W)
+    if r1 <= r0:
+        return r0, r0
+    T = -(-(r1 - r0) // stride)
+    return r0, min(r0 + T * stride, W)
+
+
+def tangent_adjoint_slabs(f, g, df, dg, lam, dlam, N, erosion, stride, rank, world, dist, op):
+    """Columns [lo, hi) of shrinkageTangentAdjointOaS's dLam_f and dLam_g.
+    f, g, df, dg: own image columns; lam, dlam: own W-sized columns.
+    op(f_h, g_h, df_h, dg_h, lam_h, dlam_h, c0, c1, dLam_f, dLam_g) gets views
+    whose row 0 is column c0 (the halos of srk_tangent_adjoint_slab around
+    them)."""
+    e = erosion
+    W = N - 2 * e
+    owns = slab_bounds(N, e, stride, world)
+    wowns = _w_owns(owns, W)
+    fneeds, gneeds, lneeds = [], [], []
+    for lo, hi in owns:
+        if lo == hi:
+            fneeds.append((lo, lo))
+            gneeds.append((lo, lo))
+            lneeds.append((0, 0))
+            continue
+        r0, rE = ta_wrange(lo, hi, N, e, stride)
+        fneeds.append(_clip(lo - e - 1, hi + e + 1, N))
+        gneeds.append(_clip(min(r0, lo), max(rE + 2 * e, lo + 1), N))
+        lneeds.append(_clip(min(lo - 2 * e, r0), max(min(hi, W), rE, lo + 1), W))
+    fh = [exchange_columns(x, owns[rank], fneeds[rank], owns, fneeds, rank, dist) for x in (f, df)]
+    gh = [exchange_columns(x, owns[rank], gneeds[rank], owns, gneeds, rank, dist) for x in (g, dg)]
+    lh = [exchange_columns(x, wowns[rank], lneeds[rank], wowns, lneeds, rank, dist) for x in (lam, dlam)]
+    lo, hi = owns[rank]
+    dlf = f.new_zeros((hi - lo, N))
+    dlg = f.new_zeros((hi - lo, N))
+    if lo < hi:
+        kf, kg, kl = lo - fneeds[rank][0], lo - gneeds[rank][0], lo - lneeds[rank][0]
+        op(fh[0][kf:], gh[0][kg:], fh[1][kf:], gh[1][kg:], lh[0][kl:], lh[1][kl:], lo, hi, dlf, dlg)
+    return dlf, dlg
+
+
 def device_slab_ops(plan, Gx, Gy, N, erosion, dx, stream=None):
-    """The device ops for forward_slabs / tangent_slabs / adjoint_slabs."""
+    """The device ops for forward_slabs / tangent_slabs / adjoint_slabs
+    (tangent_adjoint_slabs: device_tangent_adjoint_slab_op)."""
     from . import srkForwardOaSSlab, shrinkageTangentOaSSlab, adjointSRKSlab
 
     def fwd(E_h, I_h, c0, c1, R):
@@ -160,3 +206,14 @@ def device_slab_ops(plan, Gx, Gy, N, erosion, dx, stream=None):
         adjointSRKSlab(v_h, ux_h, uy_h, I_h, Gx, Gy, N, erosion, dx, c0, c1, stream, dLdI, dLdE, plan)
 
     return fwd, tan, adj
+
+
+def device_tangent_adjoint_slab_op(plan, Gx, Gy, N, erosion, dx, stream=None):
+    """The device op for tangent_adjoint_slabs."""
+    from . import shrinkageTangentAdjointOaSSlab
+
+    def tadj(f_h, g_h, df_h, dg_h, lam_h, dlam_h, c0, c1, dlf, dlg):
+        shrinkageTangentAdjointOaSSlab(f_h, g_h, df_h, dg_h, lam_h, dlam_h, Gx, Gy, N, erosion, dx, c0, c1, stream,
+                                       dlf, dlg, plan)
+
+    return tadj

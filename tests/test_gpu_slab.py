@@ -1,5 +1,5 @@
 """One image split by column slabs (srk_forward_oas_slab, srk_tangent_slab,
-srk_adjoint_slab), the per-GPU step of the multi-GPU split of a single large
+srk_adjoint_slab, srk_tangent_adjoint_slab), the per-GPU step of the multi-GPU split of a single large
 image.  The slabs of every rank are computed here one after another on one
 GPU from buffers that hold exactly the halo'd columns the C declarations
 name, between guard columns of NaN: a read outside the halo turns an output
@@ -10,7 +10,7 @@ import pytest
 
 import shrinkage_full_tests_b200 as srk
 from oracle import oracle as O
-from shrinkage_full_tests_b200.shard import slab_bounds
+from shrinkage_full_tests_b200.shard import slab_bounds, ta_wrange
 from tests.helpers import fields, kernel, pixel_violations, rel_max_err
 from tests.gpu_util import dev, host, spectra
 
@@ -52,8 +52,12 @@ def test_slabs_forward_tangent_adjoint(torch_cuda, N, KW, tile, world):
     dI = torch.zeros((N, N), device="cuda")
     dE = torch.zeros((N, N), device="cuda")
     srk.adjointSRK(v, ux, uy, f, GX, GY, N, W, e, 1.0, None, dI, dE, plan)
+    lam, dlam = (torch.randn((W, W), device="cuda", generator=gen) for _ in range(2))
+    tf = torch.zeros((N, N), device="cuda")
+    tg = torch.zeros((N, N), device="cuda")
+    srk.shrinkageTangentAdjointOaS(f, g, df, dg, lam, dlam, GX, GY, N, W, e, 1.0, None, tf, tg, plan)
     # slabs
-    sR, sdh, sdI, sdE = (torch.zeros_like(t) for t in (R, dh, dI, dE))
+    sR, sdh, sdI, sdE, stf, stg = (torch.zeros_like(t) for t in (R, dh, dI, dE, tf, tg))
     guard = tile
     for lo, hi in slab_bounds(N, e, S, world):
         if lo == hi:
@@ -65,8 +69,16 @@ def test_slabs_forward_tangent_adjoint(torch_cuda, N, KW, tile, world):
         vs = [guarded(t, max(lo - 2 * e, 0), min(hi, W), lo, guard, torch) for t in (v, ux, uy)]
         fs = guarded(f, max(lo - e - 1, 0), min(hi + e + 1, N), lo, guard, torch)
         srk.adjointSRKSlab(*vs, fs, GX, GY, N, e, 1.0, lo, hi, None, sdI[lo:], sdE[lo:], plan)
+        # tangent-adjoint: the halos of srk_tangent_adjoint_slab
+        r0, rE = ta_wrange(lo, hi, N, e, S)
+        fd = [guarded(t, max(lo - e - 1, 0), min(hi + e + 1, N), lo, guard, torch) for t in (f, df)]
+        gd = [guarded(t, r0, max(min(rE + 2 * e, N), lo + 1), lo, guard, torch) for t in (g, dg)]
+        ld = [guarded(t, min(max(lo - 2 * e, 0), r0), max(min(hi, W), rE, lo + 1), lo, guard, torch)
+              for t in (lam, dlam)]
+        srk.shrinkageTangentAdjointOaSSlab(fd[0], gd[0], fd[1], gd[1], ld[0], ld[1], GX, GY, N, e, 1.0, lo, hi, None,
+                                           stf[lo:], stg[lo:], plan)
     torch.cuda.synchronize()
-    for got, ref in ((sR, R), (sdh, dh), (sdE, dE)):
+    for got, ref in ((sR, R), (sdh, dh), (sdE, dE), (stf, tf), (stg, tg)):
         a, b = host(got), host(ref)
         assert np.isfinite(a).all()
         assert pixel_violations(a, b, tol_abs=1e-6, tol_rel=1e-4) == 0

@@ -115,12 +115,24 @@ def _slab_worker(rank, world, port, q):
         dLdI.copy_(torch.from_numpy(O.adj_wrt_I(ve, uxe, uye, N, e)[c0:c1]))
         dLdE.copy_(torch.from_numpy(O.adj_wrt_E(ve, Ie, Kx, Ky, e, 1.0, "true")[c0:c1]))
 
+    def ta_op(f_h, g_h, df_h, dg_h, lam_h, dlam_h, c0, c1, dlf, dlg):
+        emb = []
+        for t, n_cols, rows in ((f_h, N, N), (g_h, N, N), (df_h, N, N), (dg_h, N, N), (lam_h, W, W), (dlam_h, W, W)):
+            b = t._base if t._base is not None else t
+            emb.append(_embed(b.numpy(), c0 - t.storage_offset() // t.shape[1], n_cols, rows))
+        of, og = O.tangent_adjoint(*emb, Kx, Ky, e, 1.0, "true")
+        dlf.copy_(torch.from_numpy(of[c0:c1]))
+        dlg.copy_(torch.from_numpy(og[c0:c1]))
+
     R = shard.forward_slabs(T(g, lo, hi), T(f, lo, hi), N, e, S, rank, world, dist, fwd_op)
     dh = shard.tangent_slabs(T(f, lo, hi), T(g, lo, hi), T(df, lo, hi), T(dg, lo, hi), N, e, S, rank, world, dist,
                              tan_op)
     dI, dE = shard.adjoint_slabs(T(v, wlo, whi), T(ux, wlo, whi), T(uy, wlo, whi), T(f, lo, hi), N, e, S, rank,
                                  world, dist, adj_op)
-    q.put((rank, (lo, hi), R.numpy(), dh.numpy(), dI.numpy(), dE.numpy()))
+    lam, dlam = (rng.standard_normal((W, W)) for _ in range(2))
+    tf, tg = shard.tangent_adjoint_slabs(T(f, lo, hi), T(g, lo, hi), T(df, lo, hi), T(dg, lo, hi), T(lam, wlo, whi),
+                                         T(dlam, wlo, whi), N, e, S, rank, world, dist, ta_op)
+    q.put((rank, (lo, hi), R.numpy(), dh.numpy(), dI.numpy(), dE.numpy(), tf.numpy(), tg.numpy()))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -153,6 +165,10 @@ def test_column_slabs_with_halo_exchange_match_whole_image(world):
     assert np.array_equal(np.concatenate([r[3] for r in res]), O.tangent(f, g, df, dg, Kx, Ky, e, 1.0))
     assert np.array_equal(np.concatenate([r[4] for r in res]), O.adj_wrt_I(v, ux, uy, N, e))
     assert np.array_equal(np.concatenate([r[5] for r in res]), O.adj_wrt_E(v, f, Kx, Ky, e, 1.0, "true"))
+    lam, dlam = (rng.standard_normal((W, W)) for _ in range(2))
+    of, og = O.tangent_adjoint(f, g, df, dg, lam, dlam, Kx, Ky, e, 1.0, "true")
+    assert np.array_equal(np.concatenate([r[6] for r in res]), of)
+    assert np.array_equal(np.concatenate([r[7] for r in res]), og)
 
 
 def test_slab_bounds_whole_tiles():
