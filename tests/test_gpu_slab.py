@@ -1,6 +1,6 @@
 """One image split by column slabs (srk_forward_oas_slab, srk_tangent_slab,
-srk_adjoint_slab, srk_tangent_adjoint_slab), the per-GPU step of the multi-GPU split of a single large
-image.  The slabs of every rank are computed here one after another on one
+srk_adjoint_slab, srk_tangent_adjoint_slab), the per-GPU step of the
+multi-GPU split of a single large image.  The slabs of every rank are computed here one after another on one
 GPU from buffers that hold exactly the halo'd columns the C declarations
 name, between guard columns of NaN: a read outside the halo turns an output
 NaN.  The stitched slabs must match the whole-image call to rounding (work
