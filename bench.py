@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-ops", action="store_true")
     p.add_argument("--no-extra", action="store_true", help="skip the fp16 and published-config lines")
+    p.add_argument("--no-graph", action="store_true", help="time direct calls instead of the captured CUDA graph")
+    p.add_argument("--no-grid", action="store_true", help="skip the per-op grid (Mpix/s and error per size)")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--large-slabs", action="store_true",
                    help="also time one N=32768 KW=121 image split by column slabs over the ranks "
@@ -286,15 +288,33 @@ def run_ours(a):
     plan = srk.SrkPlan(N, W, e, dx, B, tile_M=a.tile_M if a.tile_M else srk.SRK_TILE_AUTOTUNE)
     if a.schedule != "auto":
         plan.set_schedule(srk.SRK_SCHEDULE_PERSISTENT if a.schedule == "persistent" else srk.SRK_SCHEDULE_THREE_PASS)
-    step = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
-    step()
+    call = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
+    call()
     plan.sync()
     info = plan.info()
+    # the step is one CUDA graph launch: the whole launch sequence of the
+    # call (P1 / P2 / P3 per scratch chunk on three streams, forked from and
+    # joined back into the capturing stream) captured once and replayed
+    graph = None
+    if not a.no_graph:
+        cs = torch.cuda.Stream()
+        cs.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(cs):
+            call()
+        cs.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=cs):
+            call()
+        torch.cuda.synchronize()
+    step = graph.replay if graph is not None else call
 
     clk = ClockSampler(local)
     clk.start()
     ms = time_steps(torch, step, a.steps, a.warmup, dist)
     clocks = clk.stop()
+    ms_direct = None
+    if graph is not None and not a.no_extra:
+        ms_direct = time_steps(torch, call, max(5, a.steps // 4), 2, dist)
     ms = max_over_ranks(torch, dist, ms)
     imgs_per_s = world * B / (ms * 1e-3)
     mpix = world * B * W * W / (ms * 1e-3) / 1e6
@@ -316,6 +336,9 @@ def run_ours(a):
     ops = None
     if not a.no_ops and world == 1:
         ops = ops_throughput(torch, srk)
+    grid = None
+    if not a.no_grid and world == 1:
+        grid = ops_grid(torch, srk)
 
     extra = {}
     if not a.no_extra and world == 1:
@@ -336,6 +359,7 @@ def run_ours(a):
         cpu = {"value": rate, "unit": "img/s", "cores": nth, "kind": "port",
                "sample": "%d images of N=%d KW=%d, FP64 direct valid convolution (oracle), %.1f s" % (n, N, KW, el)}
 
+    del graph
     if dist:
         dist.barrier()
     if rank == 0:
@@ -357,8 +381,12 @@ def run_ours(a):
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
+            "ops_grid": grid,
             "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass"][info["schedule"]],
-                         "autotuned": a.schedule == "auto"},
+                         "autotuned": a.schedule == "auto",
+                         "step": "one CUDA graph launch of the captured call" if graph is not None
+                                 else "direct call",
+                         "ms_per_step_direct_call": ms_direct},
         }
         line.update(extra)
         print(json.dumps(line))
@@ -433,6 +461,70 @@ def ops_throughput(torch, srk, N=4096, KW=61, reps=3, spectra_M=1024, ell=8.0):
         px = W * W if k in ("forward", "tangent") else N * N
         out[k] = {"ms": ms, "out_mpix_per_s": px / (ms * 1e-3) / 1e6,
                   "hbm_frac": alg[k] * 4 / (ms * 1e-3) / 1e9 / peak}
+    return out
+
+
+def ops_grid(torch, srk, reps=3):
+    """Output Mpix/s of each operator over the benchmark grid, FP32 and FP16
+    storage: forward and adjoint at N in {1k, 2k, 4k, 8k} x KW in {31, 61,
+    121}; tangent and tangent-adjoint at N in {4k, 8k, 16k} x KW in {31, 121};
+    one image per call, GRF inputs, spectra at the reference's OaS tile size
+    (1024, 2048 from N = 8k).  hbm_frac: the operator's algorithmic bytes
+    (forward 2N^2 + W^2, adjoint with v, ux, uy given 3W^2 + 3N^2, tangent
+    4N^2 + W^2, tangent-adjoint 6N^2 + 2W^2; 4 or 2 bytes per value) over the
+    time, against the measured HBM peak.  The errors of the same operators
+    against the FP64 oracle come from the GPU parity tests
+    (tests/test_gpu_configs.py), not from this timing run."""
+    peak, _ = measured_peaks()
+    cases = [(op, N, KW) for N in (1024, 2048, 4096, 8192) for KW in (31, 61, 121) for op in ("forward", "adjoint")]
+    cases += [(op, N, KW) for N in (4096, 8192, 16384) for KW in (31, 121) for op in ("tangent", "tangent_adjoint")]
+    out = []
+    by_size = {}
+    for op, N, KW in cases:
+        by_size.setdefault((N, KW), []).append(op)
+    for (N, KW), ops in sorted(by_size.items()):
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        Ms = 2048 if N >= 8192 else 1024
+        _, _, GX, GY = make_spectra(torch, srk, KW, Ms, 1.0)
+        f32 = grf_batch(torch, 2, N, 300 + N + KW)
+        gen = torch.Generator(device="cuda").manual_seed(N + KW)
+        for dt, tdt, sdt, bpv in (("f32", torch.float32, srk.SRK_F32, 4), ("f16", torch.float16, srk.SRK_F16, 2)):
+            f, g = f32[0].to(tdt), f32[1].to(tdt)
+            plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=Ms, dtype=sdt)
+            R = torch.empty((W, W), device="cuda", dtype=tdt)
+            ux, uy = torch.empty_like(R), torch.empty_like(R)
+            o1 = torch.empty((N, N), device="cuda", dtype=tdt)
+            o2 = torch.empty_like(o1)
+            lam = torch.randn((W, W), device="cuda", generator=gen).to(tdt)
+            runs, alg = {}, {}
+            if "forward" in ops:
+                runs["forward"] = lambda: srk.srkForwardOaS(g, f, GX, GY, N, W, e, 1.0, None, R, plan, ux, uy)
+                alg["forward"] = 2 * N * N + W * W
+            if "adjoint" in ops:
+                runs["adjoint"] = lambda: srk.adjointSRK(lam, ux, uy, f, GX, GY, N, W, e, 1.0, None, o1, o2, plan)
+                alg["adjoint"] = 3 * W * W + 3 * N * N
+            if "tangent" in ops:
+                df = (1e-2 * torch.randn((N, N), device="cuda", generator=gen)).to(tdt)
+                dg = (1e-2 * torch.randn((N, N), device="cuda", generator=gen)).to(tdt)
+                dlam = torch.randn((W, W), device="cuda", generator=gen).to(tdt)
+                runs["tangent"] = lambda: srk.shrinkageTangentOaS(f, g, df, dg, GX, GY, N, W, e, 1.0, None, R, plan)
+                alg["tangent"] = 4 * N * N + W * W
+                runs["tangent_adjoint"] = lambda: srk.shrinkageTangentAdjointOaS(f, g, df, dg, lam, dlam, GX, GY, N, W,
+                                                                                 e, 1.0, None, o1, o2, plan)
+                alg["tangent_adjoint"] = 6 * N * N + 2 * W * W
+            srk.srkForwardOaS(g, f, GX, GY, N, W, e, 1.0, None, R, plan, ux, uy)  # ux, uy for the adjoint
+            for op, fn in runs.items():
+                ms = time_steps(torch, fn, reps, 1, None)
+                px = W * W if op in ("forward", "tangent") else N * N
+                out.append({"op": op, "N": N, "KW": KW, "storage": dt, "ms": ms,
+                            "out_mpix_per_s": px / (ms * 1e-3) / 1e6,
+                            "hbm_frac": alg[op] * bpv / (ms * 1e-3) / 1e9 / peak,
+                            "tile_M": plan.info()["tile_M"]})
+            del plan, R, ux, uy, o1, o2, lam
+            runs.clear()
+            torch.cuda.empty_cache()
+        del f32
     return out
 
 
@@ -523,46 +615,71 @@ def cpu_checker_f32_rate(N, KW, dx, Kx, Ky, img, cols=16):
                       % (cols, W, N, KW, el)}
 
 
+def ref_inputs(torch, N, KW, dx, B, n_distinct=16):
+    """Inputs of the reference arm, made without the product library: the
+    kernel and its spectrum by the FP64 oracle on the host (make_kernel,
+    srkPrecomputeKernelFreq restated), B images cycled from `n_distinct`
+    host Gaussian random fields (the timed reference kernels do not depend
+    on the data)."""
+    import numpy as np
+    from oracle import oracle as O
+    e = (KW - 1) // 2
+    Kx, Ky = O.make_kernel(KW, dx, 1.0 / 30.0, e * dx)
+    imgs = np.stack([O.grf(N, 8.0, 17 + i).astype(np.float32) for i in range(min(B, n_distinct))])
+    base = torch.from_numpy(imgs).cuda()
+    reps = (B + base.shape[0] - 1) // base.shape[0]
+    E = base.repeat(reps, 1, 1)[:B].contiguous()
+    return Kx, Ky, E
+
+
+def ref_spectra(torch, Kx, Ky, M):
+    from oracle import oracle as O
+    return (torch.from_numpy(O.kernel_freq(Kx, M)).cuda(), torch.from_numpy(O.kernel_freq(Ky, M)).cuda())
+
+
 def gpu_reference_oas(N=4096, KW=61, M=1024, reps=5):
-    """Reference-structure stand-in for srkForwardOaS (srk_forward.cuh:354-501),
-    whose cufftDX build is unavailable (MathDx is not installed): the same
-    per-tile loop — for each of Gx, Gy and each M x M tile (stride M - 2e):
-    2-D R2C FFT, product with the kernel spectrum, C2R, valid crop — then the
-    central differences and the combine, with cuFFT (through torch.fft) as
-    the tile FFT.  Timed on this GPU with CUDA events."""
+    """Stand-in for srkForwardOaS (srk_forward.cuh:354-501), whose cufftDX
+    build is unavailable (MathDx is not installed): the same overlap-and-save
+    decomposition — M x M tiles at stride M - 2e, 2-D R2C FFT, products with
+    the Gx and Gy spectra, C2R, valid crop — with every tile of the image in
+    ONE batched cuFFT plan (torch.fft over a [tiles, M, M] batch), then the
+    central differences and the combine.  A fair lower bound for the
+    per-tile cufftDX kernels (the same FFT work, batched).  Checked against
+    the FP64 oracle on one output window; timed with CUDA events."""
     try:
+        import numpy as np
         import torch
         if not torch.cuda.is_available():
             return None
-        import shrinkage_full_tests_b200 as srk
+        from oracle import oracle as O
         e = (KW - 1) // 2
         W = N - 2 * e
         S = M - 2 * e
         T = (W + S - 1) // S
-        Kx, Ky, _, _ = make_spectra(torch, srk, KW, M, 1.0)
-        # kernel spectra in the tile frame: kernel centred at the origin (the fftshift of the reference)
+        Kx, Ky, f3 = ref_inputs(torch, N, KW, 1.0, 1)
+        f = f3[0]
+        Kxt, Kyt = torch.from_numpy(Kx).cuda(), torch.from_numpy(Ky).cuda()
+
         def spec(K):
+            # kernel centred at the origin of the tile frame (the reference's fftshift)
             P = torch.zeros((M, M), device="cuda")
             P[:KW, :KW] = K
             P = torch.roll(P, shifts=(-e, -e), dims=(0, 1))
             return torch.fft.rfft2(P)
-        SX, SY = spec(Kx), spec(Ky)
-        f = grf_batch(torch, 1, N, 77)[0]
+        SX, SY = spec(Kxt), spec(Kyt)
         pad = torch.zeros((T * S + 2 * e, T * S + 2 * e), device="cuda")
-        pad[:N, :N] = f
-        ux = torch.empty((T * S, T * S), device="cuda")
-        uy = torch.empty_like(ux)
 
         def step():
-            for G, u in ((SX, ux), (SY, uy)):
-                for tx in range(T):
-                    for ty in range(T):
-                        tile = pad[tx * S:tx * S + M, ty * S:ty * S + M]
-                        c = torch.fft.irfft2(torch.fft.rfft2(tile) * G, s=(M, M))
-                        u[tx * S:(tx + 1) * S, ty * S:(ty + 1) * S] = c[e:e + S, e:e + S]
+            pad[:N, :N] = f
+            tiles = pad.unfold(0, M, S).unfold(1, M, S).reshape(T * T, M, M)
+            F = torch.fft.rfft2(tiles)
+            u = []
+            for G in (SX, SY):
+                c = torch.fft.irfft2(F * G, s=(M, M))[:, e:e + S, e:e + S]
+                u.append(c.reshape(T, T, S, S).permute(0, 2, 1, 3).reshape(T * S, T * S)[:W, :W])
             fx = (f[e + 1:N - e + 1, e:N - e] - f[e - 1:N - e - 1, e:N - e]) * 0.5
             fy = (f[e:N - e, e + 1:N - e + 1] - f[e:N - e, e - 1:N - e - 1]) * 0.5
-            return ux[:W, :W] * fx + uy[:W, :W] * fy
+            return u[0] * fx + u[1] * fy
 
         for _ in range(2):
             step()
@@ -574,17 +691,14 @@ def gpu_reference_oas(N=4096, KW=61, M=1024, reps=5):
         s1.record()
         torch.cuda.synchronize()
         ms = s0.elapsed_time(s1) / reps
-        # the stand-in computes the same operator: compare with the library once
-        _, _, GXr, GYr = make_spectra(torch, srk, KW, M, 1.0)
-        plan = srk.SrkPlan(N, W, e, 1.0, 1, spectra_M=M)
-        R = torch.empty((W, W), device="cuda")
-        srk.srkForwardOaS(f, f, GXr, GYr, N, W, e, 1.0, None, R, plan)
-        torch.cuda.synchronize()
-        ref = step()
-        diff = float((R - ref).abs().max() / ref.abs().max())
-        return {"what": "reference-structure per-tile cuFFT stand-in for srkForwardOaS (cufftDX build unavailable)",
+        R = step().double().cpu().numpy()
+        ox = oy = W // 2
+        fh = f.double().cpu().numpy()
+        ref = O.forward(fh, fh, Kx, Ky, e, 1.0, window=(ox, oy, 128, 128))
+        diff = float(np.abs(R[ox:ox + 128, oy:oy + 128] - ref).max() / np.abs(ref).max())
+        return {"what": "srkForwardOaS stand-in: every tile in one batched cuFFT plan (cufftDX build unavailable)",
                 "config": "N=%d KW=%d M_TILE=%d, %d tiles per conv" % (N, KW, M, T * T), "ms": ms,
-                "out_mpix_per_s": W * W / (ms * 1e-3) / 1e6, "max_rel_diff_vs_library": diff}
+                "out_mpix_per_s": W * W / (ms * 1e-3) / 1e6, "max_rel_diff_vs_oracle_window": diff}
     except Exception as ex:  # noqa: BLE001
         return {"unavailable": "%s" % ex}
 
@@ -602,17 +716,16 @@ def gpu_reference_cudnn(a, B=20, reps=2):
         L = ref_gpu()
         if L is None:
             return {"unavailable": "oracle/_ref/libref_gpu.so not built"}
-        import shrinkage_full_tests_b200 as srk
         N, KW, dx = a.N, a.KW, a.dx
         e = (KW - 1) // 2
         W = N - 2 * e
-        Kx, Ky, GX, GY = make_spectra(torch, srk, KW, N, dx)
-        E = grf_batch(torch, B, N, 17)
+        Kx, Ky, E = ref_inputs(torch, N, KW, dx, B)
+        Kxt, Kyt = torch.from_numpy(Kx).cuda(), torch.from_numpy(Ky).cuda()
         R = torch.empty((B, W, W), device="cuda")
         st = torch.cuda.current_stream().cuda_stream
         ws = L.ref_cudnn_ws_create(N, W, KW, B, st)
-        call = lambda: L.ref_cudnn_forward(E.data_ptr(), E.data_ptr(), Kx.data_ptr(), Ky.data_ptr(), N, W, e, dx, B,
-                                           st, R.data_ptr(), ws)
+        call = lambda: L.ref_cudnn_forward(E.data_ptr(), E.data_ptr(), Kxt.data_ptr(), Kyt.data_ptr(), N, W, e, dx,
+                                           B, st, R.data_ptr(), ws)
         assert call() == 0
         torch.cuda.synchronize()
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -623,22 +736,17 @@ def gpu_reference_cudnn(a, B=20, reps=2):
         torch.cuda.synchronize()
         ms = s0.elapsed_time(s1) / reps
         L.ref_cudnn_ws_destroy(ws, st)
-        plan = srk.SrkPlan(N, W, e, dx, B)
-        Rl = torch.empty_like(R)
-        srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, Rl, plan)
-        torch.cuda.synchronize()
-        diff = float((Rl - R).abs().max() / R.abs().max())
         return {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "B": B,
                 "what": "reference srkCudnnForward (cuDNN heuristic algorithm) compiled for sm_100a from its sources, "
-                        "bounded batch of the same workload",
-                "max_rel_diff_vs_library": diff}
+                        "bounded batch of the same workload"}
     except Exception as ex:  # noqa: BLE001
         return {"unavailable": "%s" % ex}
 
 
 def gpu_reference(a):
     """The reference's own cuFFT srkTrainingForward (built from its sources into
-    oracle/_ref) on this GPU, same workload; None if unavailable."""
+    oracle/_ref) on this GPU, same workload; None if unavailable.  Its inputs
+    and spectra are made without the product library (ref_inputs)."""
     try:
         import torch
         if not torch.cuda.is_available():
@@ -648,12 +756,11 @@ def gpu_reference(a):
         L = ref_gpu()
         if L is None:
             return {"unavailable": "oracle/_ref/libref_gpu.so not built"}
-        import shrinkage_full_tests_b200 as srk
         N, KW, B, dx = a.N, a.KW, a.B, a.dx
         e = (KW - 1) // 2
         W = N - 2 * e
-        _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
-        E = grf_batch(torch, B, N, 17)
+        Kx, Ky, E = ref_inputs(torch, N, KW, dx, B)
+        GX, GY = ref_spectra(torch, Kx, Ky, N)
         R = torch.empty((B, W, W), device="cuda")
         free0 = torch.cuda.mem_get_info()[0]
         st = torch.cuda.current_stream().cuda_stream
@@ -664,7 +771,8 @@ def gpu_reference(a):
         ms = time_steps(torch, fn, max(2, a.steps), 1, None)
         L.ref_train_ws_destroy(ws, st)
         return {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "workspace_bytes": ws_bytes,
-                "what": "reference srkTrainingForward (cuFFT) compiled for sm_100a from its sources"}
+                "what": "reference srkTrainingForward (cuFFT) compiled for sm_100a from its sources",
+                "inputs": "16 host GRFs (FP64 oracle generator) cycled over B; spectra by the FP64 oracle"}
     except Exception as ex:  # the CPU line must still print
         return {"unavailable": "%s" % ex}
 

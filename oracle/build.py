@@ -16,7 +16,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("SRK_REFERENCE_DIR", "/root/reference")
+# The reference checkout: $SRK_REFERENCE_DIR, else a directory named
+# "reference" beside the repository (the checkout layout this recipe is
+# used with).  Nothing is built from it when neither exists.
+REF_SRC = os.environ.get("SRK_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <map>
+
 #include "../../include/srk_b200.h"
 #include "engine.cuh"
 
@@ -70,6 +72,16 @@ struct srk_plan_s {
   bool have_G = false;
   const void* src[2] = {nullptr, nullptr};
   float2* tw = nullptr;                // W_M^m, float
+  // spectrum import / set_kernel workspace, allocated with the plan so that
+  // importing spectra needs no allocation and no host synchronisation:
+  // FP64 twiddle tables at the tile size and at spectra_M, the column pass
+  // of the kernel DFT (KW x M), the spatial recovery (spectra_M/2+1 x KW)
+  // and one FP64 kernel (KW x KW), KW = 2*erosion+1
+  double2* imp_tab = nullptr;          // (cos, sin)(2 pi m / M), m < M
+  double2* imp_tabr = nullptr;         // the same at spectra_M
+  double2* imp_P = nullptr;
+  double2* imp_Tm = nullptr;
+  double* imp_Kd = nullptr;
   float2* scratch = nullptr;
   size_t scratch_bytes = 0;
   float* wbuf = nullptr;               // wx, wy for dL/df
@@ -92,13 +104,25 @@ struct srk_plan_s {
   cudaEvent_t ev_fork = nullptr;
   cudaEvent_t ev1[kRing] = {}, ev2[kRing] = {}, ev3[kRing] = {};
   bool overlap = true;
-  // ragged batches: device tables of the last ragged call (tile -> image,
-  // per-image sizes/offsets), rebuilt only when the image sizes change
+  // ragged batches and column slabs: device tile tables (tile -> image,
+  // per-image sizes/offsets), one set per key (the image sizes of a ragged
+  // batch, or a slab's kind, image and columns), built on the first call
+  // with that key and kept, so calls that alternate keys (a forward slab
+  // and an adjoint slab of one training step) reuse them and can be
+  // captured in a CUDA graph after one call of each outside the capture.
+  struct TableSet {
+    int4* tiles = nullptr;
+    srk::RagImage* imgs = nullptr;
+    int ntiles_fwd = 0, ntiles_adj = 0, nblk = 0;
+    long long sum_nn = 0, sum_ww = 0;
+    unsigned long long last_use = 0;
+  };
+  static constexpr size_t kMaxTableSets = 64;
+  std::map<std::vector<int>, TableSet> tables;
+  unsigned long long table_clock = 0;
+  // the set selected by the current call
   int4* rag_tiles = nullptr;
-  size_t rag_tiles_cap = 0;
   srk::RagImage* rag_imgs = nullptr;
-  size_t rag_imgs_cap = 0;
-  std::vector<int> rag_key;
   int rag_ntiles_fwd = 0, rag_ntiles_adj = 0, rag_nblk = 0;
   long long rag_sum_nn = 0, rag_sum_ww = 0;
 };
@@ -108,5 +132,10 @@ namespace srk {
 // Run one engine operator over all work tiles of geometry g (conv_<type>.cu).
 template <int OP, typename T>
 srk_status launch_conv(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s);
+
+// Spectrum kernels defined in spectra.cuh (compiled once, in srk_abi.cu) and
+// launched from the other translation units too.
+__global__ void k_relayout(const float2* __restrict__ ref, int M, float scale, float2* __restrict__ full);
+__global__ void k_fft_twiddles(float2* __restrict__ tw, int M);
 
 }  // namespace srk

@@ -58,35 +58,6 @@ srk_status noalloc_scratch(void** out) {
   return SRK_OK;
 }
 
-// The FFT twiddle table (per-pass blocks, tw_entry), exp(-2 pi i num/den)
-// in double, rounded once to float.
-__global__ void k_noalloc_twiddles(float2* __restrict__ tw, int M) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= M) return;
-  int num = 0, den = 1;
-  tw_entry(M, m, num, den);
-  double s, c;
-  sincospi(2.0 * (double)num / (double)den, &s, &c);
-  tw[m] = m < tw_entries(M) ? make_float2((float)c, (float)-s) : make_float2(0.f, 0.f);
-}
-
-// Reference half spectrum (size M) -> engine layout, Hermitian extension,
-// scale dx^2/M^2 (the same mapping the plans use).
-__global__ void k_noalloc_relayout(const float2* __restrict__ ref, int M, float scale, float2* __restrict__ full) {
-  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ky = blockIdx.y;
-  if (kx >= M) return;
-  const int H = M / 2 + 1;
-  float2 v;
-  if (ky <= M / 2) {
-    v = ref[(long long)kx * H + ky];
-  } else {
-    const float2 s = ref[(long long)((M - kx) % M) * H + (M - ky)];
-    v = make_float2(s.x, -s.y);
-  }
-  full[(long long)ky * M + kx] = make_float2(v.x * scale, v.y * scale);
-}
-
 }  // namespace
 
 extern "C" srk_status srk_training_forward_noalloc(const float* d_E, const float* d_I, const void* d_Gx_freq,
@@ -118,8 +89,8 @@ extern "C" srk_status srk_training_forward_noalloc(const float* d_E, const float
 
   // A plan view over the static array (host struct on the stack; nothing is allocated).
   srk_plan_s view;
-  cudaGetDevice(&view.device);
-  cudaDeviceGetAttribute(&view.nsm, cudaDevAttrMultiProcessorCount, view.device);
+  SRK_CUDA(cudaGetDevice(&view.device));
+  SRK_CUDA(cudaDeviceGetAttribute(&view.nsm, cudaDevAttrMultiProcessorCount, view.device));
   view.N = N; view.W = W; view.e = erosion; view.dx = dx; view.B_max = B; view.spectra_M = N;
   view.dtype = SRK_F32;
   view.M = M; view.S = S; view.T = 1; view.Ta = 1;
@@ -131,12 +102,12 @@ extern "C" srk_status srk_training_forward_noalloc(const float* d_E, const float
   view.scratch_bytes = (cap - fixed) * sizeof(float2);
   view.schedule = SRK_SCHEDULE_THREE_PASS;
 
-  k_noalloc_twiddles<<<(M + 127) / 128, 128, 0, s>>>(view.tw, M);
+  // the twiddles and the spectrum re-layout of the plans (same kernels, so
+  // the result equals srk_training_forward's with a plan at tile size N)
+  k_fft_twiddles<<<(M + 127) / 128, 128, 0, s>>>(view.tw, M);
   const float scale = (dx * dx) / ((float)M * (float)M);
-  k_noalloc_relayout<<<dim3((M + 127) / 128, M), 128, 0, s>>>(static_cast<const float2*>(d_Gx_freq), M, scale,
-                                                              view.G[0]);
-  k_noalloc_relayout<<<dim3((M + 127) / 128, M), 128, 0, s>>>(static_cast<const float2*>(d_Gy_freq), M, scale,
-                                                              view.G[1]);
+  k_relayout<<<dim3((M + 127) / 128, M), 128, 0, s>>>(static_cast<const float2*>(d_Gx_freq), M, scale, view.G[0]);
+  k_relayout<<<dim3((M + 127) / 128, M), 128, 0, s>>>(static_cast<const float2*>(d_Gy_freq), M, scale, view.G[1]);
   SRK_CUDA(cudaGetLastError());
 
   OpArgs a;

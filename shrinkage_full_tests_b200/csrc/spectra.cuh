@@ -12,6 +12,7 @@
 // so no angle is ever reduced in floating point.
 #pragma once
 #include <cuda_runtime.h>
+#include "fft_warp.cuh"
 
 namespace srk {
 
@@ -160,6 +161,36 @@ __global__ void k_recover_b(const double2* __restrict__ Tm, int Mr, int c, const
   const double2 tn = Tm[(long long)(Mr / 2) * KW + dxi];
   s += ((dy & 1) ? -1.0 : 1.0) * tn.x;
   Kd[idx] = s / ((double)Mr * (double)Mr);
+}
+
+
+// Double-precision twiddle table tab[m] = (cos, sin)(2 pi m / M), built on
+// the device (sincospi takes the angle as a multiple of pi, so no angle is
+// reduced in floating point): callers need no host table and no host sync.
+__global__ void k_twiddles64(double2* __restrict__ tab, int M) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  double s, c;
+  sincospi(2.0 * (double)m / (double)M, &s, &c);
+  tab[m] = make_double2(c, s);
+}
+
+// The FFT engine's float twiddle table (per-pass blocks of tw_entry):
+// exp(-2 pi i num/den) in double, rounded once to float; entries past
+// tw_entries(M) are zero.  Plans and the no-allocation forward both build
+// their tables with this kernel, so the two paths use identical twiddles.
+__global__ void k_fft_twiddles(float2* __restrict__ tw, int M) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  float2 v = make_float2(0.f, 0.f);
+  if (m < tw_entries(M)) {
+    int num = 0, den = 1;
+    tw_entry(M, m, num, den);
+    double s, c;
+    sincospi(2.0 * (double)num / (double)den, &s, &c);
+    v = make_float2((float)c, (float)-s);
+  }
+  tw[m] = v;
 }
 
 __global__ void k_float_to_double(const float* __restrict__ a, double* __restrict__ b, int n) {

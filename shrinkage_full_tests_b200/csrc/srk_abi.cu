@@ -32,16 +32,6 @@ struct NvtxRange {
   NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
-// Host double-precision twiddle table (cos, sin)(2 pi m / M).
-std::vector<double2> twiddles64(int M) {
-  std::vector<double2> t(M);
-  for (int m = 0; m < M; ++m) {
-    const double a = 2.0 * 3.14159265358979323846 * (double)m / (double)M;
-    t[m] = make_double2(std::cos(a), std::sin(a));
-  }
-  return t;
-}
-
 }  // namespace
 
 
@@ -136,29 +126,25 @@ srk_status adj_wrt_f(srk_plan_s* p, const float* wx, const float* wy, const void
 }
 
 // ---- spectra -----------------------------------------------------------------------
-srk_status upload_table(const std::vector<double2>& t, double2** d, cudaStream_t s) {
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(d), t.size() * sizeof(double2), s));
-  SRK_CUDA(cudaMemcpyAsync(*d, t.data(), t.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
-  // the host vector dies with this call: make the copy complete first
-  SRK_CUDA(cudaStreamSynchronize(s));
-  return SRK_OK;
+// FP64 twiddle table (cos, sin)(2 pi m / M) built on the device.
+srk_status build_tab64(double2* tab, int M, cudaStream_t s) {
+  k_twiddles64<<<(M + 127) / 128, 128, 0, s>>>(tab, M);
+  return cuda_status(cudaGetLastError(), "twiddle table launch");
 }
 
 // Spatial kernel (double, column-major KW x KW) -> engine spectrum at size M.
-srk_status spectrum_from_spatial(const double* Kd, int KW, int M, double scale, float2* full, float2* ref,
-                                 cudaStream_t s) {
-  double2* tab = nullptr;
-  double2* P = nullptr;
-  SRK_TRY(upload_table(twiddles64(M), &tab, s));
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&P), sizeof(double2) * (size_t)KW * M, s));
+// tab: FP64 twiddles at size M; P: KW x M double2 of workspace.
+srk_status spectrum_from_spatial(const double* Kd, int KW, int M, const double2* tab, double2* P, double scale,
+                                 float2* full, float2* ref, cudaStream_t s) {
   k_dft_cols<<<dim3((M + 127) / 128, KW), 128, 0, s>>>(Kd, KW, M, tab, P);
   k_dft_rows<<<dim3((M + 127) / 128, M), 128, 0, s>>>(P, KW, M, tab, scale, full, ref);
-  SRK_CUDA(cudaGetLastError());
-  SRK_CUDA(cudaFreeAsync(P, s));
-  SRK_CUDA(cudaFreeAsync(tab, s));
-  return SRK_OK;
+  return cuda_status(cudaGetLastError(), "kernel DFT launch");
 }
 
+// Caller spectrum (reference layout, size spectra_M) -> the plan's engine
+// layout at the tile size.  Stream-ordered; uses only the plan's import
+// workspace (no allocation, no host synchronisation), so it may run under
+// stream capture.
 srk_status import_one(srk_plan_s* p, const float2* ref, float2* full, cudaStream_t s) {
   const int Mr = p->spectra_M;
   // dx^2 / M^2 folded into the spectrum (srkConvOaS applies dx*dx/(M*M), srk_forward.cuh:380)
@@ -171,20 +157,10 @@ srk_status import_one(srk_plan_s* p, const float2* ref, float2* full, cudaStream
   // FP64, then take its spectrum at the tile size.
   const int c = p->e;
   const int KW = 2 * c + 1;
-  double2* tab = nullptr;
-  double2* Tm = nullptr;
-  double* Kd = nullptr;
-  SRK_TRY(upload_table(twiddles64(Mr), &tab, s));
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&Tm), sizeof(double2) * (size_t)(Mr / 2 + 1) * KW, s));
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&Kd), sizeof(double) * (size_t)KW * KW, s));
-  k_recover_a<<<dim3((KW + 127) / 128, Mr / 2 + 1), 128, 0, s>>>(ref, Mr, c, tab, Tm);
-  k_recover_b<<<(KW * KW + 127) / 128, 128, 0, s>>>(Tm, Mr, c, tab, Kd);
+  k_recover_a<<<dim3((KW + 127) / 128, Mr / 2 + 1), 128, 0, s>>>(ref, Mr, c, p->imp_tabr, p->imp_Tm);
+  k_recover_b<<<(KW * KW + 127) / 128, 128, 0, s>>>(p->imp_Tm, Mr, c, p->imp_tabr, p->imp_Kd);
   SRK_CUDA(cudaGetLastError());
-  SRK_TRY(spectrum_from_spatial(Kd, KW, p->M, (double)scale, full, nullptr, s));
-  SRK_CUDA(cudaFreeAsync(Tm, s));
-  SRK_CUDA(cudaFreeAsync(Kd, s));
-  SRK_CUDA(cudaFreeAsync(tab, s));
-  return SRK_OK;
+  return spectrum_from_spatial(p->imp_Kd, KW, p->M, p->imp_tab, p->imp_P, (double)scale, full, nullptr, s);
 }
 
 srk_status import_spectra(srk_plan_s* p, const void* gx, const void* gy, cudaStream_t s) {
@@ -432,16 +408,27 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
     for (cudaEvent_t* ev : {&p->ev1[r], &p->ev2[r], &p->ev3[r]})
       if ((err = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
         return cleanup(cuda_status(err, "event creation"));
-  // per-pass twiddle blocks (tw_entry), exp(-2 pi i num/den) in double, rounded once
-  std::vector<float2> tw(M, make_float2(0.f, 0.f));
-  for (int m = 0; m < tw_entries(M); ++m) {
-    int num = 0, den = 1;
-    tw_entry(M, m, num, den);
-    const double ang = 2.0 * 3.14159265358979323846 * (double)num / (double)den;
-    tw[m] = make_float2((float)std::cos(ang), (float)-std::sin(ang));
+  // spectrum import workspace (sizes in internal.h)
+  {
+    const size_t KW = 2 * (size_t)erosion + 1;
+    const size_t Mr = (size_t)spectra_M;
+    struct { void** ptr; size_t bytes; } bufs[] = {
+        {reinterpret_cast<void**>(&p->imp_tab), sizeof(double2) * (size_t)M},
+        {reinterpret_cast<void**>(&p->imp_tabr), sizeof(double2) * Mr},
+        {reinterpret_cast<void**>(&p->imp_P), sizeof(double2) * KW * (size_t)M},
+        {reinterpret_cast<void**>(&p->imp_Tm), sizeof(double2) * (Mr / 2 + 1) * KW},
+        {reinterpret_cast<void**>(&p->imp_Kd), sizeof(double) * KW * KW}};
+    for (auto& b : bufs)
+      if ((err = cudaMalloc(b.ptr, b.bytes)) != cudaSuccess) return cleanup(cuda_status(err, "import workspace"));
   }
-  if ((err = cudaMemcpy(p->tw, tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice)) != cudaSuccess)
-    return cleanup(cuda_status(err, "twiddle upload"));
+  // twiddle tables built on the device: the engine's per-pass float blocks
+  // (k_fft_twiddles, shared with the no-allocation forward) and the FP64
+  // tables of the spectrum import
+  k_fft_twiddles<<<(M + 127) / 128, 128>>>(p->tw, M);
+  k_twiddles64<<<(M + 127) / 128, 128>>>(p->imp_tab, M);
+  k_twiddles64<<<(spectra_M + 127) / 128, 128>>>(p->imp_tabr, spectra_M);
+  if ((err = cudaGetLastError()) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
+  if ((err = cudaStreamSynchronize(0)) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
   *out = p;
   return SRK_OK;
 }
@@ -449,14 +436,20 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
 srk_status srk_plan_destroy(srk_plan p) {
   if (!p) return SRK_OK;
   cudaSetDevice(p->device);
+  // work queued on any of the caller's streams may still use the plan's
+  // buffers (cudaFree would synchronise the device as well)
   cudaDeviceSynchronize();
   if (p->scratch) cudaFree(p->scratch);
   if (p->G[0]) cudaFree(p->G[0]);
   if (p->G[1]) cudaFree(p->G[1]);
   if (p->tw) cudaFree(p->tw);
+  for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd})
+    if (q) cudaFree(q);
   if (p->wbuf) cudaFree(p->wbuf);
-  if (p->rag_tiles) cudaFree(p->rag_tiles);
-  if (p->rag_imgs) cudaFree(p->rag_imgs);
+  for (auto& kv : p->tables) {
+    if (kv.second.tiles) cudaFree(kv.second.tiles);
+    if (kv.second.imgs) cudaFree(kv.second.imgs);
+  }
   if (p->ctl) cudaFree(p->ctl);
   if (p->mailbox) cudaFreeHost(p->mailbox);
   if (p->mailbox_spins) cudaFreeHost(p->mailbox_spins);
@@ -548,15 +541,12 @@ srk_status srk_plan_set_kernel(srk_plan p, const float* Kx, const float* Ky, int
   if (KW < 1 || !(KW & 1) || KW > 2 * p->e + 1)
     return fail(SRK_ERR_INVALID_ARG, "KW=%d must be odd and <= 2*erosion+1=%d", KW, 2 * p->e + 1);
   SRK_TRY(set_device(p));
-  double* Kd = nullptr;
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&Kd), sizeof(double) * KW * KW, s));
   const double scale = (double)p->dx * (double)p->dx / ((double)p->M * (double)p->M);
   const float* K[2] = {Kx, Ky};
   for (int i = 0; i < 2; ++i) {
-    k_float_to_double<<<(KW * KW + 255) / 256, 256, 0, s>>>(K[i], Kd, KW * KW);
-    SRK_TRY(spectrum_from_spatial(Kd, KW, p->M, scale, p->G[i], nullptr, s));
+    k_float_to_double<<<(KW * KW + 255) / 256, 256, 0, s>>>(K[i], p->imp_Kd, KW * KW);
+    SRK_TRY(spectrum_from_spatial(p->imp_Kd, KW, p->M, p->imp_tab, p->imp_P, scale, p->G[i], nullptr, s));
   }
-  SRK_CUDA(cudaFreeAsync(Kd, s));
   p->src[0] = p->src[1] = nullptr;
   p->have_G = true;
   return SRK_OK;
@@ -576,10 +566,19 @@ srk_status srk_precompute_kernel_freq(const float* K, int KW, int M, void* freq,
   SRK_NONNULL(freq);
   if (KW < 1 || !(KW & 1) || M < KW || (M & 1))
     return fail(SRK_ERR_INVALID_ARG, "need odd KW <= M, even M (KW=%d M=%d)", KW, M);
+  // stream-ordered temporaries (no host synchronisation): FP64 kernel,
+  // twiddle table and the column pass of the DFT
   double* Kd = nullptr;
+  double2* tab = nullptr;
+  double2* P = nullptr;
   SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&Kd), sizeof(double) * KW * KW, s));
+  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tab), sizeof(double2) * (size_t)M, s));
+  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&P), sizeof(double2) * (size_t)KW * M, s));
   k_float_to_double<<<(KW * KW + 255) / 256, 256, 0, s>>>(K, Kd, KW * KW);
-  SRK_TRY(spectrum_from_spatial(Kd, KW, M, 1.0, nullptr, static_cast<float2*>(freq), s));
+  SRK_TRY(build_tab64(tab, M, s));
+  SRK_TRY(spectrum_from_spatial(Kd, KW, M, tab, P, 1.0, nullptr, static_cast<float2*>(freq), s));
+  SRK_CUDA(cudaFreeAsync(P, s));
+  SRK_CUDA(cudaFreeAsync(tab, s));
   SRK_CUDA(cudaFreeAsync(Kd, s));
   return SRK_OK;
 }
@@ -729,39 +728,67 @@ srk_status op_jvp(const void* f, const void* g, const void* df, const void* dg, 
 }
 
 // ---- ragged batches -----------------------------------------------------------
-// Uploads the tile tables of the forward-type (`fwd`) and adjoint-type
-// (`adj`) geometries and the image table, keyed by `key` (the sizes of a
-// ragged batch, or a slab's image and columns).
+// Selects the device tile tables for `key` (the sizes of a ragged batch, or
+// a slab's kind, image and columns).  Every key keeps its own tables, built
+// on its first call: later calls with any known key upload nothing, so
+// calls that alternate keys stay cheap and can be captured in a CUDA graph.
+// A key seen for the first time while `s` is being captured is an error
+// (building tables copies from host memory, which a graph cannot replay).
+// Beyond kMaxTableSets keys the least recently used set is released
+// (stream-ordered); a graph captured with it must not be replayed after that.
+bool select_tables(srk_plan_s* p, const std::vector<int>& key) {
+  auto it = p->tables.find(key);
+  if (it == p->tables.end()) return false;
+  srk_plan_s::TableSet& t = it->second;
+  t.last_use = ++p->table_clock;
+  p->rag_tiles = t.tiles;
+  p->rag_imgs = t.imgs;
+  p->rag_ntiles_fwd = t.ntiles_fwd;
+  p->rag_ntiles_adj = t.ntiles_adj;
+  p->rag_nblk = t.nblk;
+  p->rag_sum_nn = t.sum_nn;
+  p->rag_sum_ww = t.sum_ww;
+  return true;
+}
+
+srk_status missing_tables_in_capture() {
+  return fail(SRK_ERR_UNSUPPORTED,
+              "ragged/slab tile tables for these sizes are built on their first call, which cannot happen during "
+              "stream capture: make one call with the same sizes before capturing");
+}
+
 srk_status upload_tables(srk_plan_s* p, std::vector<int> key, std::vector<int4> fwd, const std::vector<int4>& adj,
                          const std::vector<RagImage>& imgs, int nblk, long long sum_nn, long long sum_ww,
                          cudaStream_t s) {
+  if (stream_capturing(s)) return missing_tables_in_capture();
+  if (p->tables.size() >= srk_plan_s::kMaxTableSets) {
+    auto old = p->tables.begin();
+    for (auto it = p->tables.begin(); it != p->tables.end(); ++it)
+      if (it->second.last_use < old->second.last_use) old = it;
+    SRK_CUDA(cudaFreeAsync(old->second.tiles, s));
+    SRK_CUDA(cudaFreeAsync(old->second.imgs, s));
+    p->tables.erase(old);
+  }
   const size_t nt = fwd.size() + adj.size();
   const size_t B = imgs.size();
-  if (p->rag_tiles_cap < nt) {
-    if (p->rag_tiles) SRK_CUDA(cudaFreeAsync(p->rag_tiles, s));
-    p->rag_tiles = nullptr;
-    p->rag_tiles_cap = 0;
-    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_tiles), nt * sizeof(int4), s));
-    p->rag_tiles_cap = nt;
+  srk_plan_s::TableSet t;
+  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&t.tiles), std::max<size_t>(nt, 1) * sizeof(int4), s));
+  const cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&t.imgs), B * sizeof(RagImage), s);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(t.tiles, s);
+    return cuda_status(e, "tile table allocation");
   }
-  if (p->rag_imgs_cap < B) {
-    if (p->rag_imgs) SRK_CUDA(cudaFreeAsync(p->rag_imgs, s));
-    p->rag_imgs = nullptr;
-    p->rag_imgs_cap = 0;
-    SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->rag_imgs), B * sizeof(RagImage), s));
-    p->rag_imgs_cap = B;
-  }
-  const int nfwd = (int)fwd.size();
+  t.ntiles_fwd = (int)fwd.size();
+  t.ntiles_adj = (int)adj.size();
   fwd.insert(fwd.end(), adj.begin(), adj.end());
   // pageable sources: the copies have taken the data when the calls return
-  SRK_CUDA(cudaMemcpyAsync(p->rag_tiles, fwd.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, s));
-  SRK_CUDA(cudaMemcpyAsync(p->rag_imgs, imgs.data(), B * sizeof(RagImage), cudaMemcpyHostToDevice, s));
-  p->rag_key = std::move(key);
-  p->rag_ntiles_fwd = nfwd;
-  p->rag_ntiles_adj = (int)adj.size();
-  p->rag_nblk = nblk;
-  p->rag_sum_nn = sum_nn;
-  p->rag_sum_ww = sum_ww;
+  if (nt) SRK_CUDA(cudaMemcpyAsync(t.tiles, fwd.data(), nt * sizeof(int4), cudaMemcpyHostToDevice, s));
+  SRK_CUDA(cudaMemcpyAsync(t.imgs, imgs.data(), B * sizeof(RagImage), cudaMemcpyHostToDevice, s));
+  t.nblk = nblk;
+  t.sum_nn = sum_nn;
+  t.sum_ww = sum_ww;
+  p->tables[key] = t;
+  select_tables(p, key);
   return SRK_OK;
 }
 
@@ -780,7 +807,7 @@ srk_status ragged_tables(srk_plan_s* p, int B, const int* Ns, cudaStream_t s) {
   for (int b = 0; b < B; ++b)
     if (Ns[b] < 2 * e + 1 || Ns[b] > p->N)
       return fail(SRK_ERR_INVALID_ARG, "image %d: N=%d outside [2*erosion+1=%d, plan N=%d]", b, Ns[b], 2 * e + 1, p->N);
-  if (key == p->rag_key) return SRK_OK;
+  if (select_tables(p, key)) return SRK_OK;
   std::vector<int4> fwd, adj;
   std::vector<RagImage> imgs(B);
   long long on = 0, ow = 0, blk = 0;
@@ -825,7 +852,7 @@ srk_status slab_tables(srk_plan_s* p, int N, int c0, int c1, bool adj, cudaStrea
     return fail(SRK_ERR_INVALID_ARG, "slab [%d, %d) must span whole tiles of %d columns or end at column %d", c0, c1,
                 S, Wo);
   std::vector<int> key = {adj ? -2 : -1, N, c0, c1};
-  if (key == p->rag_key) return SRK_OK;
+  if (select_tables(p, key)) return SRK_OK;
   std::vector<int4> tiles;
   for (int x0 = c0; x0 < c1; x0 += S)
     for (int y0 = 0; y0 < Wo; y0 += S) tiles.push_back(make_int4(0, x0, y0, 0));
@@ -863,7 +890,7 @@ srk_status slab_tables_ta(srk_plan_s* p, int N, int c0, int c1, int* r0o, int* r
   *r0o = r0;
   *rEo = T ? std::min(r0 + T * S, W) : r0;
   std::vector<int> key = {-3, N, c0, c1};
-  if (key == p->rag_key) return SRK_OK;
+  if (select_tables(p, key)) return SRK_OK;
   std::vector<int4> fwd, adj;
   for (int k = 0; k < T; ++k)
     for (int y0 = 0; y0 < W; y0 += S) fwd.push_back(make_int4(0, r0 + k * S, y0, 0));

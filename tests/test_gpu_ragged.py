@@ -12,6 +12,7 @@ import shrinkage_full_tests_b200 as srk
 from oracle import oracle as O
 from tests.helpers import fields, kernel, pixel_violations, rel_max_err
 from tests.gpu_util import dev, host, spectra
+from tests.windows import adjoint_window, windows
 
 pytestmark = pytest.mark.gpu
 
@@ -133,7 +134,9 @@ def test_ragged_tangent_and_tangent_adjoint(torch_cuda):
 
 def test_ragged_adjoint_sixteen_large_images(torch_cuda):
     """Sixteen images with N drawn from {1k, 2k, 4k, 8k}, KW = 61, one ragged
-    adjoint call, against the single-image calls."""
+    adjoint call, against the single-image calls and, for every distinct
+    size, the FP64 oracle on two 128 x 128 output windows (one at the image's
+    last pixels)."""
     torch = torch_cuda
     KW, tile = 61, 512
     Ns = [int(n) for n in np.random.default_rng(2026).choice([1024, 2048, 4096, 8192], 16)]
@@ -165,6 +168,14 @@ def test_ragged_adjoint_sixteen_large_images(torch_cuda):
             a, r = host(dLdE[on:on + n * n]).reshape(n, n), host(sE)
             assert pixel_violations(a, r, tol_abs=1e-6, tol_rel=1e-4) == 0, b
             del p1, sI, sE
+            img = lambda t, o, m: t[o:o + m * m].view(m, m)
+            for px, py in windows(n, 128, 1, n, corners=False) + [(n - 128, n - 128)]:
+                (gi, ri), (ge, re) = adjoint_window(img(v, ow, w), img(ux, ow, w), img(uy, ow, w), img(f, on, n),
+                                                    Kx, Ky, e, 1.0, img(dLdI, on, n), img(dLdE, on, n), px, py,
+                                                    128, "reference")
+                assert rel_max_err(gi, ri) < 1e-5, (b, px, py)
+                assert rel_max_err(ge, re) < 1e-4, (b, px, py)
+                assert pixel_violations(ge, re) == 0, (b, px, py)
         on += n * n
         ow += w * w
 

@@ -18,16 +18,18 @@ from tests.helpers import fields, kernel, pixel_violations, rel_max_err
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(L, E, GX, GY, N, W, e, dx, B, R, stream):
+def _noalloc(L, E, I, GX, GY, N, W, e, dx, B, R, stream):
     fn = L.srk_training_forward_noalloc
     fn.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
                                            ctypes.c_void_p, ctypes.c_void_p]
     fn.restype = ctypes.c_int
-    return fn(E.data_ptr(), E.data_ptr(), GX.data_ptr(), GY.data_ptr(), N, W, e, dx, B, stream, R.data_ptr())
+    return fn(E.data_ptr(), I.data_ptr(), GX.data_ptr(), GY.data_ptr(), N, W, e, dx, B, stream, R.data_ptr())
 
 
-@pytest.mark.parametrize("N,KW,B", [(256, 31, 5), (512, 121, 13)])
+@pytest.mark.parametrize("N,KW,B", [(128, 15, 3), (256, 31, 5), (512, 121, 13)])
 def test_noalloc_matches_plan_forward_twice(torch_cuda, N, KW, B):
+    """E (convolved) and I (differentiated) are different fields, so a
+    swapped or ignored I changes the result."""
     torch = torch_cuda
     L = srk.lib()
     e = (KW - 1) // 2
@@ -38,10 +40,11 @@ def test_noalloc_matches_plan_forward_twice(torch_cuda, N, KW, B):
     plan = srk.SrkPlan(N, W, e, 4.0, B)
     for call, seed in enumerate((11, 29)):
         E = dev(np.stack(fields(N, B, seed)), torch)
+        I = dev(np.stack(fields(N, B, seed + 1000)), torch)
         R_plan = torch.zeros((B, W, W), device="cuda")
-        srk.srkTrainingForward(E, E, GX, GY, N, W, e, 4.0, B, None, R_plan, plan)
+        srk.srkTrainingForward(E, I, GX, GY, N, W, e, 4.0, B, None, R_plan, plan)
         R = torch.full((B, W, W), float("nan"), device="cuda")
-        st = _noalloc(L, E, GX, GY, N, W, e, 4.0, B, R, stream)
+        st = _noalloc(L, E, I, GX, GY, N, W, e, 4.0, B, R, stream)
         assert st == srk.SRK_OK, L.srk_last_error()
         torch.cuda.synchronize()
         a, b = host(R), host(R_plan)
@@ -57,6 +60,6 @@ def test_noalloc_rejects_unsupported_sizes(torch_cuda):
     E = torch.zeros((1, 300, 300), device="cuda")
     R = torch.zeros((1, 270, 270), device="cuda")
     G = torch.zeros((300, 151), dtype=torch.complex64, device="cuda")
-    st = _noalloc(L, E, G, G, 300, 270, 15, 1.0, 1, R, torch.cuda.current_stream().cuda_stream)
+    st = _noalloc(L, E, E, G, G, 300, 270, 15, 1.0, 1, R, torch.cuda.current_stream().cuda_stream)
     assert st == srk.SRK_ERR_UNSUPPORTED
     assert b"N in {128, 256, 512}" in L.srk_last_error()
