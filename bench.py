@@ -359,6 +359,7 @@ def run_ours(a):
         cpu = {"value": rate, "unit": "img/s", "cores": nth, "kind": "port",
                "sample": "%d images of N=%d KW=%d, FP64 direct valid convolution (oracle), %.1f s" % (n, N, KW, el)}
 
+    graphed = graph is not None
     del graph
     if dist:
         dist.barrier()
@@ -384,8 +385,7 @@ def run_ours(a):
             "ops_grid": grid,
             "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass"][info["schedule"]],
                          "autotuned": a.schedule == "auto",
-                         "step": "one CUDA graph launch of the captured call" if graph is not None
-                                 else "direct call",
+                         "step": "one CUDA graph launch of the captured call" if graphed else "direct call",
                          "ms_per_step_direct_call": ms_direct},
         }
         line.update(extra)
