@@ -63,7 +63,16 @@ typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_
  * intermediates in an L2-resident ring (falls back to THREE_PASS when the
  * scratch holds fewer than three work tiles).  SRK_TILE_AUTOTUNE plans time
  * both and keep the faster. */
-typedef enum srk_schedule { SRK_SCHEDULE_PERSISTENT = 0, SRK_SCHEDULE_THREE_PASS = 1 } srk_schedule;
+typedef enum srk_schedule { SRK_SCHEDULE_PERSISTENT = 0, SRK_SCHEDULE_THREE_PASS = 1, SRK_SCHEDULE_DIRECT = 2 } srk_schedule;
+/* SRK_SCHEDULE_DIRECT: the training forward and srk_forward run as a direct
+ * convolution on the tensor cores (tcgen05.mma, FP32 accumulation; FP16/BF16
+ * storage in one pass, FP32 storage in three passes over an exact FP16
+ * hi + lo split) instead of FFTs: (128 + KW - 1) * KW * 2 multiply-adds per
+ * output pixel, so it only pays for small kernels.  Needs erosion >= 1,
+ * 2*erosion+1 <= 63 and N % 8 == 0; the other operators keep the
+ * three-pass FFT schedule.  The counterpart of the reference's cuDNN
+ * forward (training/srk_cudnn_forward.cuh:194-269); SRK_TILE_AUTOTUNE
+ * times it against the FFT schedules where it applies. */
 
 typedef struct srk_plan_info {
   int N, W, erosion, B_max, spectra_M;

@@ -82,6 +82,14 @@ struct srk_plan_s {
   double2* imp_P = nullptr;
   double2* imp_Tm = nullptr;
   double* imp_Kd = nullptr;
+  // the bound kernels in space, FP64, on the full (2e+1)^2 support, centred
+  // (recovered from the caller's spectra, or given to srk_plan_set_kernel)
+  double* kd[2] = {nullptr, nullptr};
+  // tensor-core direct schedule (direct.cu): FP16/BF16 band tables of the
+  // bound kernels, a device error word written by its bounded waits
+  uint16_t* direct_tabs = nullptr;
+  bool direct_ready = false;
+  unsigned int* direct_err = nullptr;  // [0] error word, [1] the band tables' power-of-two exponent
   float2* scratch = nullptr;
   size_t scratch_bytes = 0;
   float* wbuf = nullptr;               // wx, wy for dL/df
@@ -132,6 +140,12 @@ namespace srk {
 // Run one engine operator over all work tiles of geometry g (conv_<type>.cu).
 template <int OP, typename T>
 srk_status launch_conv(srk_plan_s* p, const OpArgs& a, const Geom& g, bool conjG, cudaStream_t s);
+
+// Tensor-core direct convolution of the forward (direct.cu).
+bool direct_supported(const srk_plan_s* p, int N, std::string* why);
+size_t direct_tab_bytes(const srk_plan_s* p);
+srk_status direct_build_tables(srk_plan_s* p, int kern, cudaStream_t s);
+srk_status direct_forward(srk_plan_s* p, const void* E, const void* I, void* R, int B, cudaStream_t s);
 
 // Spectrum kernels defined in spectra.cuh (compiled once, in srk_abi.cu) and
 // launched from the other translation units too.

@@ -193,6 +193,15 @@ __global__ void k_fft_twiddles(float2* __restrict__ tw, int M) {
   tw[m] = v;
 }
 
+// A KW x KW float kernel centred on a KWp x KWp support (KWp >= KW, both
+// odd), in double, zero elsewhere; column-major both.
+__global__ void k_pad_centre(const float* __restrict__ K, int KW, int KWp, double* __restrict__ out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= KWp * KWp) return;
+  const int i = idx / KWp - (KWp - KW) / 2, j = idx - (idx / KWp) * KWp - (KWp - KW) / 2;
+  out[idx] = (i >= 0 && i < KW && j >= 0 && j < KW) ? (double)K[i * KW + j] : 0.0;
+}
+
 __global__ void k_float_to_double(const float* __restrict__ a, double* __restrict__ b, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i];

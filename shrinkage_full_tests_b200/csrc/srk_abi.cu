@@ -142,35 +142,47 @@ srk_status spectrum_from_spatial(const double* Kd, int KW, int M, const double2*
 }
 
 // Caller spectrum (reference layout, size spectra_M) -> the plan's engine
-// layout at the tile size.  Stream-ordered; uses only the plan's import
-// workspace (no allocation, no host synchronisation), so it may run under
-// stream capture.
-srk_status import_one(srk_plan_s* p, const float2* ref, float2* full, cudaStream_t s) {
+// layout at the tile size, and the kernel in space (kd[k], FP64, on its
+// (2e+1)^2 support) for the direct schedule.  Stream-ordered; uses only the
+// plan's import workspace (no allocation, no host synchronisation), so it
+// may run under stream capture.
+srk_status import_one(srk_plan_s* p, int k, const float2* ref, float2* full, cudaStream_t s) {
   const int Mr = p->spectra_M;
   // dx^2 / M^2 folded into the spectrum (srkConvOaS applies dx*dx/(M*M), srk_forward.cuh:380)
   const float scale = (p->dx * p->dx) / ((float)p->M * (float)p->M);
+  const int c = p->e;
+  const int KW = 2 * c + 1;
+  // spatial recovery on the kernel support, in FP64
+  k_recover_a<<<dim3((KW + 127) / 128, Mr / 2 + 1), 128, 0, s>>>(ref, Mr, c, p->imp_tabr, p->imp_Tm);
+  k_recover_b<<<(KW * KW + 127) / 128, 128, 0, s>>>(p->imp_Tm, Mr, c, p->imp_tabr, p->kd[k]);
+  SRK_CUDA(cudaGetLastError());
   if (Mr == p->M) {
+    // same FFT size: the caller's values as they are
     k_relayout<<<dim3((Mr + 127) / 128, Mr), 128, 0, s>>>(ref, Mr, scale, full);
     return cuda_status(cudaGetLastError(), "relayout");
   }
-  // Different FFT size: recover the spatial kernel on its (2e+1)^2 support in
-  // FP64, then take its spectrum at the tile size.
-  const int c = p->e;
-  const int KW = 2 * c + 1;
-  k_recover_a<<<dim3((KW + 127) / 128, Mr / 2 + 1), 128, 0, s>>>(ref, Mr, c, p->imp_tabr, p->imp_Tm);
-  k_recover_b<<<(KW * KW + 127) / 128, 128, 0, s>>>(p->imp_Tm, Mr, c, p->imp_tabr, p->imp_Kd);
-  SRK_CUDA(cudaGetLastError());
-  return spectrum_from_spatial(p->imp_Kd, KW, p->M, p->imp_tab, p->imp_P, (double)scale, full, nullptr, s);
+  // different FFT size: the spectrum of the recovered kernel at the tile size
+  return spectrum_from_spatial(p->kd[k], KW, p->M, p->imp_tab, p->imp_P, (double)scale, full, nullptr, s);
+}
+
+// Band tables of the direct schedule from kd (when it is selected).
+srk_status refresh_direct(srk_plan_s* p, cudaStream_t s) {
+  p->direct_ready = false;
+  if (p->schedule != SRK_SCHEDULE_DIRECT || !p->have_G) return SRK_OK;
+  SRK_TRY(direct_build_tables(p, 0, s));
+  SRK_TRY(direct_build_tables(p, 1, s));
+  p->direct_ready = true;
+  return SRK_OK;
 }
 
 srk_status import_spectra(srk_plan_s* p, const void* gx, const void* gy, cudaStream_t s) {
   if (!gx || !gy) return fail(SRK_ERR_INVALID_ARG, "kernel spectra are NULL");
-  SRK_TRY(import_one(p, static_cast<const float2*>(gx), p->G[0], s));
-  SRK_TRY(import_one(p, static_cast<const float2*>(gy), p->G[1], s));
+  SRK_TRY(import_one(p, 0, static_cast<const float2*>(gx), p->G[0], s));
+  SRK_TRY(import_one(p, 1, static_cast<const float2*>(gy), p->G[1], s));
   p->src[0] = gx;
   p->src[1] = gy;
   p->have_G = true;
-  return SRK_OK;
+  return refresh_direct(p, s);
 }
 
 srk_status bind_spectra(srk_plan_s* p, const void* gx, const void* gy, cudaStream_t s) {
@@ -417,7 +429,10 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
         {reinterpret_cast<void**>(&p->imp_tabr), sizeof(double2) * Mr},
         {reinterpret_cast<void**>(&p->imp_P), sizeof(double2) * KW * (size_t)M},
         {reinterpret_cast<void**>(&p->imp_Tm), sizeof(double2) * (Mr / 2 + 1) * KW},
-        {reinterpret_cast<void**>(&p->imp_Kd), sizeof(double) * KW * KW}};
+        {reinterpret_cast<void**>(&p->imp_Kd), sizeof(double) * KW * KW},
+        {reinterpret_cast<void**>(&p->kd[0]), sizeof(double) * KW * KW},
+        {reinterpret_cast<void**>(&p->kd[1]), sizeof(double) * KW * KW},
+        {reinterpret_cast<void**>(&p->direct_err), 2 * sizeof(unsigned int)}};
     for (auto& b : bufs)
       if ((err = cudaMalloc(b.ptr, b.bytes)) != cudaSuccess) return cleanup(cuda_status(err, "import workspace"));
   }
@@ -427,8 +442,15 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   k_fft_twiddles<<<(M + 127) / 128, 128>>>(p->tw, M);
   k_twiddles64<<<(M + 127) / 128, 128>>>(p->imp_tab, M);
   k_twiddles64<<<(spectra_M + 127) / 128, 128>>>(p->imp_tabr, spectra_M);
+  if ((err = cudaMemset(p->direct_err, 0, 2 * sizeof(unsigned int))) != cudaSuccess)
+    return cleanup(cuda_status(err, "error word"));
   if ((err = cudaGetLastError()) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
   if ((err = cudaStreamSynchronize(0)) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
+  if (sched == SRK_SCHEDULE_DIRECT) {
+    // the tuner chose the direct schedule for the forward
+    const srk_status st = srk_plan_set_schedule(p, SRK_SCHEDULE_DIRECT);
+    if (st != SRK_OK) return cleanup(st);
+  }
   *out = p;
   return SRK_OK;
 }
@@ -443,7 +465,8 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->G[0]) cudaFree(p->G[0]);
   if (p->G[1]) cudaFree(p->G[1]);
   if (p->tw) cudaFree(p->tw);
-  for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd})
+  for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd,
+                  (void*)p->kd[0], (void*)p->kd[1], (void*)p->direct_tabs, (void*)p->direct_err})
     if (q) cudaFree(q);
   if (p->wbuf) cudaFree(p->wbuf);
   for (auto& kv : p->tables) {
@@ -477,9 +500,22 @@ srk_status srk_plan_get_info(srk_plan p, srk_plan_info* info) {
 
 srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
-  if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS)
+  if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS && sch != SRK_SCHEDULE_DIRECT)
     return fail(SRK_ERR_INVALID_ARG, "bad schedule %d", (int)sch);
+  if (sch == SRK_SCHEDULE_DIRECT) {
+    std::string why;
+    if (!direct_supported(p, p->N, &why)) return fail(SRK_ERR_UNSUPPORTED, "direct schedule: %s", why.c_str());
+    SRK_TRY(set_device(p));
+    SRK_CUDA(cudaDeviceSynchronize());  // the bound kernel (kd) may still be in flight on the caller's stream
+    if (!p->direct_tabs) SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->direct_tabs), direct_tab_bytes(p)));
+    p->schedule = sch;
+    // band tables of an already bound kernel (legacy stream, then ready)
+    SRK_TRY(refresh_direct(p, nullptr));
+    SRK_CUDA(cudaStreamSynchronize(nullptr));
+    return SRK_OK;
+  }
   p->schedule = sch;
+  p->direct_ready = false;
   return SRK_OK;
 }
 
@@ -497,6 +533,15 @@ srk_status srk_plan_sync(srk_plan p, srk_stream_t s) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
   SRK_TRY(set_device(p));
   SRK_CUDA(cudaStreamSynchronize(s));
+  if (p->direct_err) {
+    unsigned int derr = 0;
+    SRK_CUDA(cudaMemcpy(&derr, p->direct_err, sizeof(derr), cudaMemcpyDeviceToHost));
+    if (derr) {
+      SRK_CUDA(cudaMemset(p->direct_err, 0, sizeof(derr)));
+      return fail(SRK_ERR_TIMEOUT, "a bounded wait of the direct schedule gave up (site %u); outputs incomplete",
+                  derr);
+    }
+  }
   if (p->graph_mailbox && p->mailbox[0]) {
     // written by a persistent launch replayed from a captured graph
     const unsigned int where = p->mailbox[1];
@@ -543,13 +588,15 @@ srk_status srk_plan_set_kernel(srk_plan p, const float* Kx, const float* Ky, int
   SRK_TRY(set_device(p));
   const double scale = (double)p->dx * (double)p->dx / ((double)p->M * (double)p->M);
   const float* K[2] = {Kx, Ky};
+  const int KWp = 2 * p->e + 1;
   for (int i = 0; i < 2; ++i) {
-    k_float_to_double<<<(KW * KW + 255) / 256, 256, 0, s>>>(K[i], p->imp_Kd, KW * KW);
-    SRK_TRY(spectrum_from_spatial(p->imp_Kd, KW, p->M, p->imp_tab, p->imp_P, scale, p->G[i], nullptr, s));
+    // the kernel centred on the plan's full (2e+1)^2 support
+    k_pad_centre<<<(KWp * KWp + 255) / 256, 256, 0, s>>>(K[i], KW, KWp, p->kd[i]);
+    SRK_TRY(spectrum_from_spatial(p->kd[i], KWp, p->M, p->imp_tab, p->imp_P, scale, p->G[i], nullptr, s));
   }
   p->src[0] = p->src[1] = nullptr;
   p->have_G = true;
-  return SRK_OK;
+  return refresh_direct(p, s);
 }
 
 srk_status srk_green_tensor(float* Kx, float* Ky, int KW, double gamma, double R_w, double dx, srk_stream_t s) {
@@ -599,6 +646,7 @@ srk_status op_training_forward(const void* E, const void* I, const void* gx, con
     return fail(SRK_ERR_INVALID_ARG, "training spectra must be at size N=%d (plan has spectra_M=%d)", N, p->spectra_M);
   SRK_TRY(enter(p, s));
   SRK_TRY(bind_spectra(p, gx, gy, s));
+  if (p->schedule == SRK_SCHEDULE_DIRECT) return direct_forward(p, E, I, R, B, s);
   OpArgs a = base_args(p);
   a.E = E; a.I = I; a.out0 = R;
   return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, B), false, s);
@@ -683,6 +731,7 @@ srk_status op_forward(const void* f, const void* g, int B, srk_stream_t s, void*
   SRK_NONNULL(h);
   if (!p->have_G) return fail(SRK_ERR_INVALID_ARG, "no kernel set on the plan");
   SRK_TRY(enter(p, s));
+  if (p->schedule == SRK_SCHEDULE_DIRECT) return direct_forward(p, g, f, h, B, s);
   OpArgs a = base_args(p);
   a.E = g; a.I = f; a.out0 = h;
   return launch_conv_dt<OP_FWD>(p, a, fwd_geom(p, B), false, s);
@@ -1329,6 +1378,29 @@ srk_status srk_autotune(int N, int W, int erosion, float dx, int B, srk_dtype dt
     }
   }
   if (bestM == 0) return done(fail(SRK_ERR_UNSUPPORTED, "no tile size fits erosion=%d", erosion));
+  {
+    // the tensor-core direct schedule of the forward, where it applies
+    srk_plan p = nullptr;
+    if (srk_plan_create(&p, N, W, erosion, dx, Bt, N + (N & 1), dtype, bestM, 0) == SRK_OK) {
+      std::string why;
+      if (direct_supported(p, N, &why) && srk_plan_set_schedule(p, SRK_SCHEDULE_DIRECT) == SRK_OK &&
+          (st = srk_plan_set_kernel(p, Kx, Ky, KW, s)) == SRK_OK) {
+        for (int it = 0; it < 2; ++it) op_forward(E, E, Bt, s, R, p);
+        cudaEventRecord(e0, s);
+        for (int it = 0; it < 3; ++it) op_forward(E, E, Bt, s, R, p);
+        cudaEventRecord(e1, s);
+        st = srk_plan_sync(p, s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (st == SRK_OK && ms < best) {
+          best = ms;
+          bestS = SRK_SCHEDULE_DIRECT;
+        }
+      }
+      srk_plan_destroy(p);
+      if (st != SRK_OK) return done(st);
+    }
+  }
   *tile_M = bestM;
   *schedule = bestS;
   tune_store(key, bestM, bestS);
