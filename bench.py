@@ -53,8 +53,10 @@ def parse():
     p.add_argument("--large-slabs", action="store_true",
                    help="also time one N=32768 KW=121 image split by column slabs over the ranks "
                         "(halo exchange + slab forward / adjoint)")
-    p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass"],
+    p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass", "direct"],
                    help="override the autotuned kernel schedule (profiling)")
+    p.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"],
+                   help="storage type of the main workload (profiling; the metric is quoted on f32)")
     p.add_argument("--tile-M", type=int, default=0,
                    help="fixed tile size instead of the autotuned one (profiling: no tuner launches)")
     return p.parse_args()
@@ -283,11 +285,14 @@ def run_ours(a):
     e = (KW - 1) // 2
     W = N - 2 * e
     _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
-    E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17)
-    R = torch.empty((B, W, W), device="cuda")
-    plan = srk.SrkPlan(N, W, e, dx, B, tile_M=a.tile_M if a.tile_M else srk.SRK_TILE_AUTOTUNE)
+    tdt, sdt = {"f32": (torch.float32, srk.SRK_F32), "f16": (torch.float16, srk.SRK_F16),
+                "bf16": (torch.bfloat16, srk.SRK_BF16)}[a.dtype]
+    E = grf_batch(torch, B, N, seed0=1_000_003 * rank + 17).to(tdt)
+    R = torch.empty((B, W, W), device="cuda", dtype=tdt)
+    plan = srk.SrkPlan(N, W, e, dx, B, dtype=sdt, tile_M=a.tile_M if a.tile_M else srk.SRK_TILE_AUTOTUNE)
     if a.schedule != "auto":
-        plan.set_schedule(srk.SRK_SCHEDULE_PERSISTENT if a.schedule == "persistent" else srk.SRK_SCHEDULE_THREE_PASS)
+        plan.set_schedule({"persistent": srk.SRK_SCHEDULE_PERSISTENT, "three_pass": srk.SRK_SCHEDULE_THREE_PASS,
+                           "direct": srk.SRK_SCHEDULE_DIRECT}[a.schedule])
     call = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
     call()
     plan.sync()
@@ -311,22 +316,27 @@ def run_ours(a):
     clk = ClockSampler(local)
     clk.start()
     ms = time_steps(torch, step, a.steps, a.warmup, dist)
+    # the same K steps as direct calls (15 launches each): the value is the
+    # faster of the two ways of issuing the identical work
+    ms_direct = time_steps(torch, call, a.steps, a.warmup, dist) if graph is not None else None
     clocks = clk.stop()
-    ms_direct = None
-    if graph is not None and not a.no_extra:
-        ms_direct = time_steps(torch, call, max(5, a.steps // 4), 2, dist)
+    ms_graph = ms
+    if ms_direct is not None:
+        ms_direct = max_over_ranks(torch, dist, ms_direct)
+        ms_graph = max_over_ranks(torch, dist, ms_graph)
+        ms = min(ms_graph, ms_direct)
     ms = max_over_ranks(torch, dist, ms)
     imgs_per_s = world * B / (ms * 1e-3)
     mpix = world * B * W * W / (ms * 1e-3) / 1e6
 
     launches_per_step = info["last_launches"]
     peak, peak_kind = measured_peaks()
-    alg_bytes = B * (N * N + W * W) * 4
+    alg_bytes = B * (N * N + W * W) * (4 if a.dtype == "f32" else 2)
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     traffic = profiled_traffic(N, KW, B)
 
     e2e = None
-    if not a.no_e2e:
+    if not a.no_e2e and a.dtype == "f32":
         ms_e2e, h2d, d2h = e2e_pipeline(torch, srk, plan, GX, GY, N, W, e, dx, B, max(2, a.steps // 2),
                                         1, dist)
         ms_e2e = max_over_ranks(torch, dist, ms_e2e)
@@ -342,10 +352,12 @@ def run_ours(a):
 
     extra = {}
     if not a.no_extra and world == 1:
-        extra["fp16_storage"] = half_storage_rate(torch, srk, E, GX, GY, N, W, e, dx, B)
+        extra["fp16_storage"] = half_storage_rate(torch, srk, E.float(), GX, GY, N, W, e, dx, B)
         extra["published_config"] = published_config_rate(torch, srk)
         # the large single image of the configurations: N = 32768, KW = 121, GRF ell = 32 px
         extra["large_image"] = ops_throughput(torch, srk, N=32768, KW=121, reps=1, spectra_M=2048, ell=32.0)
+        torch.cuda.empty_cache()
+        extra["direct_path"] = direct_path_rates(torch, srk)
         torch.cuda.empty_cache()
 
     if a.large_slabs:
@@ -368,7 +380,7 @@ def run_ours(a):
             "metric": "srkTrainingForward images/s (B=5000 per GPU, N=512, KW=121)",
             "value": imgs_per_s, "unit": "img/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic: seeded Gaussian random fields (ell=8 px, [0,1]), device-resident",
+            "dtype": a.dtype, "data": "synthetic: seeded Gaussian random fields (ell=8 px, [0,1]), device-resident",
             "config": {"workload": "srkTrainingForward B=%d N=%d KW=%d W=%d dx=%g nm gamma=1/30 nm" % (B, N, KW, W, dx),
                        "B_per_gpu": B, "N": N, "KW": KW, "W": W, "tile_M": info["tile_M"],
                        "l2": "inputs (%.1f GB/GPU) larger than L2; no flush" % (B * N * N * 4 / 1e9),
@@ -383,9 +395,11 @@ def run_ours(a):
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
             "ops_grid": grid,
-            "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass"][info["schedule"]],
+            "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass", "direct"][info["schedule"]],
                          "autotuned": a.schedule == "auto",
-                         "step": "one CUDA graph launch of the captured call" if graphed else "direct call",
+                         "step": ("one CUDA graph launch of the captured call" if graphed and ms == ms_graph
+                                  else "direct call (15 launches)"),
+                         "ms_per_step_graph_replay": ms_graph if graphed else None,
                          "ms_per_step_direct_call": ms_direct},
         }
         line.update(extra)
@@ -407,6 +421,54 @@ def half_storage_rate(torch, srk, E32, GX, GY, N, W, e, dx, B, steps=20):
            "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "tile_M": plan.info()["tile_M"]}
     del E, R, plan
     torch.cuda.empty_cache()
+    return out
+
+
+def direct_path_rates(torch, srk, steps=10, bf16_peak=None):
+    """The tensor-core direct schedule (SRK_SCHEDULE_DIRECT) against the FFT
+    three-pass schedule on the training forward, B = 5000, N = 256, dx = 4 nm,
+    KW = 15 and 31, FP16 storage (one MMA pass) and FP32 storage (three
+    passes).  roofline: the MMA work the kernel executes (2 kernels x KW x
+    (128 + KW - 1, rounded to 16) x 128 x 128 multiply-adds per 128 x 128
+    output tile, x 3 passes for FP32) over the time, against the measured
+    dense bf16 tensor peak; useful_tflops counts only the 2 x KW^2 taps per
+    output pixel."""
+    try:
+        path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak = float(json.load(open(path))["bf16_tflops"]) if os.path.exists(path) else 1590.0
+    except Exception:  # noqa: BLE001
+        peak = 1590.0
+    out = []
+    B, N, dx = 5000, 256, 4.0
+    E32 = grf_batch(torch, B, N, 41)
+    for KW in (15, 31):
+        e = (KW - 1) // 2
+        W = N - 2 * e
+        _, _, GX, GY = make_spectra(torch, srk, KW, N, dx)
+        tiles = B * ((W + 127) // 128) ** 2
+        KT = (128 + KW - 1 + 15) // 16 * 16
+        mma_flop = tiles * 2 * KW * KT * 128 * 128 * 2
+        useful = B * W * W * 2 * KW * KW * 2
+        for dt, sdt, tdt, npass in (("f16", srk.SRK_F16, torch.float16, 1), ("f32", srk.SRK_F32, torch.float32, 3)):
+            E = E32.to(tdt)
+            R = torch.empty((B, W, W), device="cuda", dtype=tdt)
+            row = {"N": N, "KW": KW, "B": B, "storage": dt}
+            for name, sch in (("fft_three_pass", srk.SRK_SCHEDULE_THREE_PASS), ("direct", srk.SRK_SCHEDULE_DIRECT)):
+                plan = srk.SrkPlan(N, W, e, dx, B, dtype=sdt)
+                plan.set_schedule(sch)
+                fn = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
+                ms = time_steps(torch, fn, steps, 3, None)
+                plan.sync()
+                row[name + "_ms"] = ms
+                del plan
+            tf = mma_flop * npass / (row["direct_ms"] * 1e-3) / 1e12
+            row["direct_roofline"] = {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                                      "frac": tf / peak, "peak_source": "measured bf16 dense (burst)"}
+            row["direct_useful_tflops"] = useful / (row["direct_ms"] * 1e-3) / 1e12
+            row["faster"] = "direct" if row["direct_ms"] < row["fft_three_pass_ms"] else "fft_three_pass"
+            out.append(row)
+            del E, R
+    del E32
     return out
 
 
