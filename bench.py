@@ -398,7 +398,7 @@ def run_ours(a):
             "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass", "direct"][info["schedule"]],
                          "autotuned": a.schedule == "auto",
                          "step": ("one CUDA graph launch of the captured call" if graphed and ms == ms_graph
-                                  else "direct call (15 launches)"),
+                                  else "direct call (%d launches)" % launches_per_step),
                          "ms_per_step_graph_replay": ms_graph if graphed else None,
                          "ms_per_step_direct_call": ms_direct},
         }
