@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--large-slabs", action="store_true",
                    help="also time one N=32768 KW=121 image split by column slabs over the ranks "
                         "(halo exchange + slab forward / adjoint)")
-    p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass", "direct"],
+    p.add_argument("--schedule", default="auto", choices=["auto", "persistent", "three_pass", "direct", "tensor_rows"],
                    help="override the autotuned kernel schedule (profiling)")
     p.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"],
                    help="storage type of the main workload (profiling; the metric is quoted on f32)")
@@ -292,7 +292,7 @@ def run_ours(a):
     plan = srk.SrkPlan(N, W, e, dx, B, dtype=sdt, tile_M=a.tile_M if a.tile_M else srk.SRK_TILE_AUTOTUNE)
     if a.schedule != "auto":
         plan.set_schedule({"persistent": srk.SRK_SCHEDULE_PERSISTENT, "three_pass": srk.SRK_SCHEDULE_THREE_PASS,
-                           "direct": srk.SRK_SCHEDULE_DIRECT}[a.schedule])
+                           "direct": srk.SRK_SCHEDULE_DIRECT, "tensor_rows": srk.SRK_SCHEDULE_TENSOR_ROWS}[a.schedule])
     call = lambda: srk.srkTrainingForward(E, E, GX, GY, N, W, e, dx, B, None, R, plan)
     call()
     plan.sync()
@@ -395,7 +395,8 @@ def run_ours(a):
             "gpu_launches": launches_per_step * a.steps,
             "ops": ops,
             "ops_grid": grid,
-            "schedule": {"tile_M": info["tile_M"], "schedule": ["persistent", "three_pass", "direct"][info["schedule"]],
+            "schedule": {"tile_M": info["tile_M"],
+                         "schedule": ["persistent", "three_pass", "direct", "tensor_rows"][info["schedule"]],
                          "autotuned": a.schedule == "auto",
                          "step": ("one CUDA graph launch of the captured call" if graphed and ms == ms_graph
                                   else "direct call (%d launches)" % launches_per_step),

@@ -63,7 +63,22 @@ typedef enum srk_adj_convention { SRK_ADJ_REFERENCE = 0, SRK_ADJ_TRUE = 1 } srk_
  * intermediates in an L2-resident ring (falls back to THREE_PASS when the
  * scratch holds fewer than three work tiles).  SRK_TILE_AUTOTUNE plans time
  * both and keep the faster. */
-typedef enum srk_schedule { SRK_SCHEDULE_PERSISTENT = 0, SRK_SCHEDULE_THREE_PASS = 1, SRK_SCHEDULE_DIRECT = 2 } srk_schedule;
+typedef enum srk_schedule {
+  SRK_SCHEDULE_PERSISTENT = 0,
+  SRK_SCHEDULE_THREE_PASS = 1,
+  SRK_SCHEDULE_DIRECT = 2,
+  SRK_SCHEDULE_TENSOR_ROWS = 3
+} srk_schedule;
+/* SRK_SCHEDULE_TENSOR_ROWS (FP16/BF16 storage plans at tile 512, erosion
+ * 1..64): the three-pass schedule with its row pass on the tensor cores —
+ * after the column FFT, the convolution along x is applied per frequency
+ * row as a banded complex matrix product (tcgen05.mma, FP16 operands:
+ * the column spectra are stored as FP16, FP32 accumulation) instead of the
+ * row FFT, spectral product and inverse row FFT.  Used by the forward-type
+ * operators (training forward, forward, tangent, VJP and tangent-adjoint
+ * dL/df parts); the adjoint-type pass keeps the FFT row pass.  The plan
+ * allocates the FP16 spectra planes (1 MB per work tile of its scratch)
+ * when the schedule is set. */
 /* SRK_SCHEDULE_DIRECT: the training forward and srk_forward run as a direct
  * convolution on the tensor cores (tcgen05.mma, FP32 accumulation; FP16/BF16
  * storage in one pass, FP32 storage in three passes over an exact FP16

@@ -28,7 +28,7 @@ LIB_PATH = os.environ.get("SRK_B200_LIB") or os.path.join(_PKG, "libsrk_b200.so"
 SRK_OK, SRK_ERR_INVALID_ARG, SRK_ERR_UNSUPPORTED, SRK_ERR_ALLOC, SRK_ERR_TIMEOUT, SRK_ERR_CUDA = range(6)
 SRK_F32, SRK_F16, SRK_BF16 = 0, 1, 2
 SRK_ADJ_REFERENCE, SRK_ADJ_TRUE = 0, 1
-SRK_SCHEDULE_PERSISTENT, SRK_SCHEDULE_THREE_PASS, SRK_SCHEDULE_DIRECT = 0, 1, 2
+SRK_SCHEDULE_PERSISTENT, SRK_SCHEDULE_THREE_PASS, SRK_SCHEDULE_DIRECT, SRK_SCHEDULE_TENSOR_ROWS = 0, 1, 2, 3
 
 
 class SrkError(RuntimeError):

@@ -2,6 +2,7 @@
 // operator and storage type; included by conv_<type>.cu only.
 #pragma once
 #include "internal.h"
+#include "hybrid_p1.cuh"
 
 namespace srk {
 
@@ -12,8 +13,72 @@ srk_status set_smem(K kernel, size_t bytes) {
   return SRK_OK;
 }
 
+// Three-pass schedule with the tensor-core row pass (SRK_SCHEDULE_TENSOR_ROWS):
+// P1h (column FFT -> FP16 planes), the row pass of hybrid.cu (-> S2), P3
+// unchanged; the same ring of scratch slots and streams as launch_conv_m.
+template <int OP, typename T>
+srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, cudaStream_t s) {
+  constexpr int M = kHybM;
+  constexpr int LPU = lpu_of<M>();
+  const size_t per = wt_elems<M, OP>(g.S);
+  const size_t s1 = s1_elems<M, OP>();
+  const size_t plane_wt = (size_t)2 * M * M;  // halves per work tile
+  const size_t cap = std::min<size_t>(p->scratch_bytes / sizeof(float2) / per, p->hyb_s1_bytes / sizeof(__half) / plane_wt);
+  const size_t smp1 = p1h_smem_bytes();
+  const size_t sm3 = phase_smem_bytes<M>() + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
+  SRK_TRY(set_smem(k_p1h<OP, T>, smp1));
+  SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
+  auto launch3 = [&](int w0, int c, float2* base, __half* planes, cudaStream_t s1s, cudaStream_t s2s,
+                     cudaStream_t s3s, cudaEvent_t e1, cudaEvent_t e2) -> srk_status {
+    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, s1s>>>(a, g, p->tw, w0, planes, c, p->nsm);
+    if (e1) {
+      SRK_CUDA(cudaEventRecord(e1, s1s));
+      SRK_CUDA(cudaStreamWaitEvent(s2s, e1, 0));
+    }
+    SRK_TRY(tensor_rows_p2(p, planes, c, base, per, s1, g.S, s2_pitch(g.S), s2s));
+    if (e2) {
+      SRK_CUDA(cudaEventRecord(e2, s2s));
+      SRK_CUDA(cudaStreamWaitEvent(s3s, e2, 0));
+    }
+    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s3s>>>(base, a, g, p->tw, w0, p->nsm);
+    return SRK_OK;
+  };
+  const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
+  int launches = 0;
+  constexpr int R = srk_plan_s::kRing;
+  if (nwt <= whole || !p->overlap || !p->ps1 || cap < (size_t)R) {
+    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 3)
+      SRK_TRY(launch3(w0, std::min(whole, nwt - w0), p->scratch, p->hyb_s1, s, s, s, nullptr, nullptr));
+  } else {
+    // the ring of launch_conv_m (P1h of chunk k after the row pass of chunk
+    // k-R has read its planes; the row pass after P3 of chunk k-R has read
+    // the slot's S2)
+    const int chunk = (int)std::min<size_t>(cap / R, 65535);
+    SRK_CUDA(cudaEventRecord(p->ev_fork, s));
+    SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev_fork, 0));
+    SRK_CUDA(cudaStreamWaitEvent(p->ps3, p->ev_fork, 0));
+    int k = 0;
+    for (int w0 = 0; w0 < nwt; w0 += chunk, ++k, launches += 3) {
+      const int r = k % R;
+      if (k >= R) {
+        SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev2[r], 0));
+        SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[r], 0));
+      }
+      SRK_TRY(launch3(w0, std::min(chunk, nwt - w0), p->scratch + r * (size_t)chunk * per,
+                      p->hyb_s1 + r * (size_t)chunk * plane_wt, p->ps1, s, p->ps3, p->ev1[r], p->ev2[r]));
+      SRK_CUDA(cudaEventRecord(p->ev3[r], p->ps3));
+    }
+    SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[(k - 1) % R], 0));
+  }
+  p->last_launches = launches;
+  return cuda_status(cudaGetLastError(), "tensor-row launch");
+}
+
 template <int M, int OP, typename T>
 srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, bool conjG, cudaStream_t s) {
+  if constexpr (M == kHybM && OpTraits<OP>::K == 1 && !std::is_same<T, float>::value) {
+    if (p->schedule == SRK_SCHEDULE_TENSOR_ROWS && p->hyb_ready) return launch_tensor_rows<OP, T>(p, a, g, nwt, s);
+  }
   constexpr int K = OpTraits<OP>::K;
   constexpr int L = OpTraits<OP>::L;
   const size_t sm1 = phase_smem_bytes<M>();

@@ -1,0 +1,314 @@
+// hybrid.cu — the row pass (P2) of SRK_SCHEDULE_TENSOR_ROWS on the
+// 5th-generation tensor cores, for FP16/BF16 storage plans at tile M = 512.
+//
+// After the column FFT along y (P1), the convolution along x is, for every
+// frequency row ky, a 1-D convolution with a short complex kernel:
+//   U_G[ky][x'] = sum_x g_{G,ky}[x' - x] Z[ky][x],  |x' - x| <= e,
+//   g_{G,ky}[d] = sum_kx G[ky][kx] exp(+2 pi i d kx / M)
+// where G is the plan's engine-layout spectrum (dx^2/M^2 folded in) — exactly
+// the row FFT, spectral product and inverse row FFT of the FFT row pass
+// (engine.cuh phase2) for the valid outputs, without the transforms.  The
+// inverse column FFT and the epilogue (P3) are unchanged: U is written to S2
+// in P3's blocked FP32 layout.
+//
+// GEMM form per CTA (one ky, 128 outputs x' = e + 128 j .. , 64 work tiles):
+//   D[m][n] = sum_k T[m][k] Z_n[ky][128 j + k],  T[m][k] = g[m - k + e],
+// complex: Ur = Tr Zr - Ti Zi, Ui = Tr Zi + Ti Zr, four real MMAs per K step
+// and field (the minus sign by the instruction descriptor's negate-A bit).
+// * B (Z planes, FP16, written by k_p1h) by TMA: box {8 columns x, 128 work
+//   tiles, 1 plane}, one box per 16-byte K chunk — the K-major operand.
+// * A (the band T) never materialised: rows reversed, one slot table of
+//   KT/8 + 16 slots x 128 bytes per (ky, field, part), read through a
+//   descriptor with leading = stride byte offset = 128 (direct.cu explains the
+//   identity).  Tables scaled by a power of two (max |g| in [8, 16)).
+// * Accumulators: 4 x 64 TMEM columns (Gx re/im, Gy re/im); two CTAs per
+//   SM, so one CTA's epilogue (its S2 stores) overlaps the other's loads
+//   and MMAs.
+// * Precision: FP16 operands (Z and g rounded once), FP32 accumulation — for
+//   the FP16/BF16 storage forms (rel 1e-2 / abs 1e-3).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "internal.h"
+#include "tc.cuh"
+
+namespace srk {
+namespace hyb {
+using namespace srk::tc;
+
+constexpr int M = 512;
+constexpr int MT = 128;        // outputs x' per tile = TMEM lanes
+constexpr int NB = 64;         // work tiles per MMA (N): 2 CTAs per SM (4 x 64 TMEM columns each)
+constexpr int kThreadsH = 192;
+constexpr int kMaxE = 64;
+
+__host__ __device__ constexpr int kt_of(int e) { return ((MT + 2 * e) + 15) / 16 * 16; }  // input columns per tile
+__host__ __device__ constexpr int qs_of(int e) { return kt_of(e) / 8 + MT / 8; }           // band slots
+
+struct Args {
+  const uint16_t* tabs;   // [M ky][2 field][2 part][QS][8][8] FP16 bits
+  const int* tab_exp;     // tables hold g * 2^tab_exp
+  float2* scratch;        // chunk base: S2 of work tile wl at scratch + wl*per + s1
+  size_t per, s1;         // float2 per work tile, offset of S2 in it
+  unsigned int* err;
+  unsigned long long spin_limit;
+  int c, e, S, P;         // work tiles in the chunk, erosion, valid stride, S2 pitch
+};
+
+__host__ __device__ inline size_t smem_bytes(int e) {
+  const size_t bpart = (size_t)(kt_of(e) / 8) * NB * 16;
+  return 1024 + 2 * bpart + 4 * (size_t)qs_of(e) * 128;
+}
+
+__global__ void __launch_bounds__(kThreadsH, 2) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int e = a.e, KT = kt_of(e), KC = KT / 8, QS = qs_of(e);
+  const uint32_t lboB = (uint32_t)NB * 16;      // bytes between 8-column chunks of B
+  const uint32_t bpart = (uint32_t)KC * lboB;   // one part (re / im) of the B tile
+  const uint32_t tab = (uint32_t)QS * 128;      // one (field, part) band
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* accfull = full + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accfull + 1);
+  unsigned char* Bs = smem + 1024;
+  unsigned char* As = Bs + 2 * bpart;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j = blockIdx.x, ky = blockIdx.y;
+  const int xk0 = MT * j;          // first input column of the tile's band
+  const int wl0 = NB * blockIdx.z; // first work tile of the batch
+  const unsigned long long lim = a.spin_limit;
+
+  if (threadIdx.x == 0) {
+    mbar_init(full, 1);
+    mbar_init(accfull, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(4 * NB));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      mbar_expect_tx(full, 2 * bpart + 4 * tab);
+      for (int part = 0; part < 2; ++part)
+        for (int cc = 0; cc < KC; ++cc)
+          tma_load_3d(Bs + part * bpart + cc * lboB, &zmap, xk0 + 8 * cc, wl0, ky * 2 + part, full);
+      bulk_g2s(As, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, full);
+      // every copy has landed before the CTA can leave (also on the error path)
+      mbar_wait(full, 0, lim);
+    }
+    __syncwarp();
+  } else if (warp == 5) {
+    if (lane == 0) {
+      const uint32_t id = idesc_f16(0, MT, NB);
+      const uint32_t idn = id | (1u << 13);  // negate A
+      if (!mbar_wait(full, 0, lim)) {
+        atomicCAS(a.err, 0u, 11u);
+      } else {
+        tc_fence_after();
+        const uint32_t b0 = smem_u32(Bs), a0 = smem_u32(As);
+        for (int ks = 0; ks < KT / 16; ++ks) {
+          const uint64_t dbr = sdesc(b0 + (uint32_t)ks * 2 * lboB, lboB, 128);
+          const uint64_t dbi = sdesc(b0 + bpart + (uint32_t)ks * 2 * lboB, lboB, 128);
+#pragma unroll
+          for (int f = 0; f < 2; ++f) {
+            const uint64_t dar = sdesc(a0 + (uint32_t)(f * 2 + 0) * tab + (uint32_t)ks * 256, 128, 128);
+            const uint64_t dai = sdesc(a0 + (uint32_t)(f * 2 + 1) * tab + (uint32_t)ks * 256, 128, 128);
+            const uint32_t dr = tmem + (uint32_t)(f * 2 + 0) * NB, di = tmem + (uint32_t)(f * 2 + 1) * NB;
+            mma_f16(dr, dar, dbr, id, ks > 0);   // + Tr Zr
+            mma_f16(dr, dai, dbi, idn, true);    // - Ti Zi
+            mma_f16(di, dar, dbi, id, ks > 0);   // + Tr Zi
+            mma_f16(di, dai, dbr, id, true);     // + Ti Zr
+          }
+        }
+      }
+      mma_commit(accfull);
+    }
+    __syncwarp();
+  } else {
+    bool ok = true;
+    if (lane == 0) ok = mbar_wait(accfull, 0, lim);
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    if (!ok && lane == 0) atomicCAS(a.err, 0u, 12u);
+    if (ok) {
+      tc_fence_after();
+      const int mrow = warp * 32 + lane;            // TMEM lane (rows reversed)
+      const int xv = MT * j + MT - 1 - mrow;        // valid-column index x' - e
+      const float sc = ldexpf(1.f, -__ldg(a.tab_exp));
+      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+      const size_t fo = (size_t)a.P * M;            // S2 field stride
+      const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)ky * 4 + (xv & 3);
+      for (int n0 = 0; n0 < NB; n0 += 16) {
+        float r0[16], i0[16], r1[16], i1[16];
+        tmem_ld16(trow + 0 * NB + (uint32_t)n0, r0);
+        tmem_ld16(trow + 1 * NB + (uint32_t)n0, i0);
+        tmem_ld16(trow + 2 * NB + (uint32_t)n0, r1);
+        tmem_ld16(trow + 3 * NB + (uint32_t)n0, i1);
+        tmem_wait_ld();
+        if (xv >= a.S) continue;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int wl = wl0 + n0 + k;
+          if (wl >= a.c) break;
+          float2* s2 = a.scratch + (size_t)wl * a.per + a.s1 + xo;
+          __stcg(s2, make_float2(r0[k] * sc, i0[k] * sc));
+          __stcg(s2 + fo, make_float2(r1[k] * sc, i1[k] * sc));
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * NB));
+  }
+}
+
+// g_{G,ky}[d] for d = -e .. e from the engine-layout spectra (FP32 values,
+// FP64 sums): gbuf[(f * M + ky) * (2e+1) + d + e].
+__global__ void k_hyb_g(const float2* __restrict__ Gx, const float2* __restrict__ Gy, int e,
+                        const double2* __restrict__ tab, double2* __restrict__ gbuf) {
+  const int KW = 2 * e + 1;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= 2 * M * KW) return;
+  const int f = idx / (M * KW), rem = idx - f * M * KW;
+  const int ky = rem / KW, d = rem - (rem / KW) * KW - e;
+  const float2* G = (f == 0 ? Gx : Gy) + (size_t)ky * M;
+  double re = 0.0, im = 0.0;
+  for (int kx = 0; kx < M; ++kx) {
+    const float2 v = G[kx];
+    int m = (d * kx) % M;
+    if (m < 0) m += M;
+    const double2 w = tab[m];  // (cos, sin)(2 pi m / M): exp(+i ...)
+    re += (double)v.x * w.x - (double)v.y * w.y;
+    im += (double)v.x * w.y + (double)v.y * w.x;
+  }
+  gbuf[idx] = make_double2(re, im);
+}
+
+// Power of two with 2^exp * max|g| in [8, 16).  One block.
+__global__ void k_hyb_scale(const double2* __restrict__ gbuf, int n, int* __restrict__ exp_out) {
+  __shared__ double red[256];
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, fmax(fabs(gbuf[i].x), fabs(gbuf[i].y)));
+  red[threadIdx.x] = mx;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    int e2 = 0;
+    if (red[0] > 0.0) {
+      frexp(red[0], &e2);
+      e2 = 4 - e2;
+    }
+    *exp_out = e2 < -60 ? -60 : (e2 > 60 ? 60 : e2);
+  }
+}
+
+// tabs[ky][f][part][q][r][t] = part of g_{f,ky}[e - jj] * 2^exp, jj = 8q + r + t - 127
+// (zero off the band).
+__global__ void k_hyb_tabs(const double2* __restrict__ gbuf, const int* __restrict__ exp_in, int e,
+                           uint16_t* __restrict__ tabs) {
+  const int KW = 2 * e + 1, QS = qs_of(e);
+  const long long total = (long long)M * 4 * QS * 64;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  const int w = (int)(idx % (QS * 64));
+  const long long blk = idx / (QS * 64);  // ky * 4 + f * 2 + part
+  const int part = (int)(blk & 1), f = (int)((blk >> 1) & 1), ky = (int)(blk >> 2);
+  const int q = w / 64, r = (w / 8) % 8, t = w % 8;
+  const int jj = 8 * q + r + t - (MT - 1);
+  double v = 0.0;
+  if (jj >= 0 && jj < KW) {
+    const double2 gv = gbuf[((size_t)f * M + ky) * KW + (e - jj) + e];
+    v = ldexp(part ? gv.y : gv.x, *exp_in);
+  }
+  tabs[idx] = __half_as_ushort(__double2half(v));
+}
+
+}  // namespace hyb
+
+// ---- host side ------------------------------------------------------------------------------
+bool tensor_rows_supported(const srk_plan_s* p, std::string* why) {
+  char buf[160];
+  if (p->dtype == SRK_F32) snprintf(buf, sizeof buf, "needs FP16 or BF16 storage (FP16 operands)");
+  else if (p->M != hyb::M) snprintf(buf, sizeof buf, "needs tile M = 512 (plan has %d)", p->M);
+  else if (p->e < 1 || p->e > hyb::kMaxE) snprintf(buf, sizeof buf, "needs 1 <= erosion <= %d", hyb::kMaxE);
+  else return true;
+  if (why) *why = buf;
+  return false;
+}
+
+size_t tensor_rows_tab_bytes(const srk_plan_s* p) { return (size_t)hyb::M * 4 * hyb::qs_of(p->e) * 128; }
+size_t tensor_rows_g_bytes(const srk_plan_s* p) { return sizeof(double2) * 2 * hyb::M * (2 * p->e + 1); }
+
+// Band tables from the plan's engine-layout spectra (stream-ordered).
+srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s) {
+  const int KW = 2 * p->e + 1;
+  const int n = 2 * hyb::M * KW;
+  int* exp_slot = reinterpret_cast<int*>(p->direct_err + 2);
+  hyb::k_hyb_g<<<(n + 127) / 128, 128, 0, s>>>(p->G[0], p->G[1], p->e, p->imp_tab, p->hyb_g);
+  hyb::k_hyb_scale<<<1, 256, 0, s>>>(p->hyb_g, n, exp_slot);
+  const long long total = (long long)hyb::M * 4 * hyb::qs_of(p->e) * 64;
+  hyb::k_hyb_tabs<<<(int)((total + 255) / 256), 256, 0, s>>>(p->hyb_g, exp_slot, p->e, p->hyb_tabs);
+  return cuda_status(cudaGetLastError(), "tensor-row tables");
+}
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn_h() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+}  // namespace
+
+// The row pass of one chunk of c work tiles: planes [2M][c][M] FP16 (k_p1h)
+// -> S2 of every work tile at scratch + wl*per + s1 (P3's layout).
+srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
+                          int P, cudaStream_t s) {
+  auto enc = encode_fn_h();
+  if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[3] = {(cuuint64_t)hyb::M, (cuuint64_t)c, (cuuint64_t)(2 * hyb::M)};
+  const cuuint64_t strides[2] = {(cuuint64_t)hyb::M * 2, (cuuint64_t)c * hyb::M * 2};
+  const cuuint32_t box[3] = {8, (cuuint32_t)hyb::NB, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<__half*>(planes), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  hyb::Args a;
+  a.tabs = p->hyb_tabs;
+  a.tab_exp = reinterpret_cast<const int*>(p->direct_err + 2);
+  a.scratch = scratch;
+  a.per = per;
+  a.s1 = s1;
+  a.err = p->direct_err;
+  a.spin_limit = 1ull << 22;
+  a.c = c;
+  a.e = p->e;
+  a.S = S;
+  a.P = P;
+  const size_t sm = hyb::smem_bytes(p->e);
+  SRK_CUDA(cudaFuncSetAttribute(hyb::k_p2h, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const dim3 grid((S + hyb::MT - 1) / hyb::MT, hyb::M, (c + hyb::NB - 1) / hyb::NB);
+  hyb::k_p2h<<<grid, hyb::kThreadsH, sm, s>>>(map, a);
+  return cuda_status(cudaGetLastError(), "tensor-row pass launch");
+}
+
+}  // namespace srk

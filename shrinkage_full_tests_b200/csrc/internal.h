@@ -89,7 +89,15 @@ struct srk_plan_s {
   // bound kernels, a device error word written by its bounded waits
   uint16_t* direct_tabs = nullptr;
   bool direct_ready = false;
-  unsigned int* direct_err = nullptr;  // [0] error word, [1] the band tables' power-of-two exponent
+  unsigned int* direct_err = nullptr;  // [0] error word, [1] / [2] the direct / tensor-row tables' exponents
+  // tensor-core row pass (hybrid.cu, SRK_SCHEDULE_TENSOR_ROWS): FP16 column
+  // spectra planes of the chunks in flight, the band tables per ky, the FP64
+  // row kernels they are made from
+  __half* hyb_s1 = nullptr;
+  size_t hyb_s1_bytes = 0;
+  uint16_t* hyb_tabs = nullptr;
+  double2* hyb_g = nullptr;
+  bool hyb_ready = false;
   float2* scratch = nullptr;
   size_t scratch_bytes = 0;
   float* wbuf = nullptr;               // wx, wy for dL/df
@@ -146,6 +154,14 @@ bool direct_supported(const srk_plan_s* p, int N, std::string* why);
 size_t direct_tab_bytes(const srk_plan_s* p);
 srk_status direct_build_tables(srk_plan_s* p, int kern, cudaStream_t s);
 srk_status direct_forward(srk_plan_s* p, const void* E, const void* I, void* R, int B, cudaStream_t s);
+
+// Tensor-core row pass of the FP16/BF16 forms at tile 512 (hybrid.cu).
+bool tensor_rows_supported(const srk_plan_s* p, std::string* why);
+size_t tensor_rows_tab_bytes(const srk_plan_s* p);
+size_t tensor_rows_g_bytes(const srk_plan_s* p);
+srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s);
+srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
+                          int P, cudaStream_t s);
 
 // Spectrum kernels defined in spectra.cuh (compiled once, in srk_abi.cu) and
 // launched from the other translation units too.

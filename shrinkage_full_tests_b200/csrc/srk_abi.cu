@@ -165,13 +165,20 @@ srk_status import_one(srk_plan_s* p, int k, const float2* ref, float2* full, cud
   return spectrum_from_spatial(p->kd[k], KW, p->M, p->imp_tab, p->imp_P, (double)scale, full, nullptr, s);
 }
 
-// Band tables of the direct schedule from kd (when it is selected).
+// Band tables of the tensor-core schedules from the bound kernel (when one
+// of them is selected).
 srk_status refresh_direct(srk_plan_s* p, cudaStream_t s) {
   p->direct_ready = false;
-  if (p->schedule != SRK_SCHEDULE_DIRECT || !p->have_G) return SRK_OK;
-  SRK_TRY(direct_build_tables(p, 0, s));
-  SRK_TRY(direct_build_tables(p, 1, s));
-  p->direct_ready = true;
+  p->hyb_ready = false;
+  if (!p->have_G) return SRK_OK;
+  if (p->schedule == SRK_SCHEDULE_DIRECT) {
+    SRK_TRY(direct_build_tables(p, 0, s));
+    SRK_TRY(direct_build_tables(p, 1, s));
+    p->direct_ready = true;
+  } else if (p->schedule == SRK_SCHEDULE_TENSOR_ROWS) {
+    SRK_TRY(tensor_rows_build_tables(p, s));
+    p->hyb_ready = true;
+  }
   return SRK_OK;
 }
 
@@ -432,7 +439,7 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
         {reinterpret_cast<void**>(&p->imp_Kd), sizeof(double) * KW * KW},
         {reinterpret_cast<void**>(&p->kd[0]), sizeof(double) * KW * KW},
         {reinterpret_cast<void**>(&p->kd[1]), sizeof(double) * KW * KW},
-        {reinterpret_cast<void**>(&p->direct_err), 2 * sizeof(unsigned int)}};
+        {reinterpret_cast<void**>(&p->direct_err), 4 * sizeof(unsigned int)}};
     for (auto& b : bufs)
       if ((err = cudaMalloc(b.ptr, b.bytes)) != cudaSuccess) return cleanup(cuda_status(err, "import workspace"));
   }
@@ -442,13 +449,13 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
   k_fft_twiddles<<<(M + 127) / 128, 128>>>(p->tw, M);
   k_twiddles64<<<(M + 127) / 128, 128>>>(p->imp_tab, M);
   k_twiddles64<<<(spectra_M + 127) / 128, 128>>>(p->imp_tabr, spectra_M);
-  if ((err = cudaMemset(p->direct_err, 0, 2 * sizeof(unsigned int))) != cudaSuccess)
+  if ((err = cudaMemset(p->direct_err, 0, 4 * sizeof(unsigned int))) != cudaSuccess)
     return cleanup(cuda_status(err, "error word"));
   if ((err = cudaGetLastError()) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
   if ((err = cudaStreamSynchronize(0)) != cudaSuccess) return cleanup(cuda_status(err, "twiddle tables"));
-  if (sched == SRK_SCHEDULE_DIRECT) {
-    // the tuner chose the direct schedule for the forward
-    const srk_status st = srk_plan_set_schedule(p, SRK_SCHEDULE_DIRECT);
+  if (sched == SRK_SCHEDULE_DIRECT || sched == SRK_SCHEDULE_TENSOR_ROWS) {
+    // the tuner chose a tensor-core schedule for the forward
+    const srk_status st = srk_plan_set_schedule(p, (srk_schedule)sched);
     if (st != SRK_OK) return cleanup(st);
   }
   *out = p;
@@ -466,7 +473,8 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->G[1]) cudaFree(p->G[1]);
   if (p->tw) cudaFree(p->tw);
   for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd,
-                  (void*)p->kd[0], (void*)p->kd[1], (void*)p->direct_tabs, (void*)p->direct_err})
+                  (void*)p->kd[0], (void*)p->kd[1], (void*)p->direct_tabs, (void*)p->direct_err,
+                  (void*)p->hyb_s1, (void*)p->hyb_tabs, (void*)p->hyb_g})
     if (q) cudaFree(q);
   if (p->wbuf) cudaFree(p->wbuf);
   for (auto& kv : p->tables) {
@@ -500,8 +508,27 @@ srk_status srk_plan_get_info(srk_plan p, srk_plan_info* info) {
 
 srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
   if (!p) return fail(SRK_ERR_INVALID_ARG, "plan is NULL");
-  if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS && sch != SRK_SCHEDULE_DIRECT)
+  if (sch != SRK_SCHEDULE_PERSISTENT && sch != SRK_SCHEDULE_THREE_PASS && sch != SRK_SCHEDULE_DIRECT &&
+      sch != SRK_SCHEDULE_TENSOR_ROWS)
     return fail(SRK_ERR_INVALID_ARG, "bad schedule %d", (int)sch);
+  if (sch == SRK_SCHEDULE_TENSOR_ROWS) {
+    std::string why;
+    if (!tensor_rows_supported(p, &why)) return fail(SRK_ERR_UNSUPPORTED, "tensor-row schedule: %s", why.c_str());
+    SRK_TRY(set_device(p));
+    SRK_CUDA(cudaDeviceSynchronize());  // the bound spectra may still be in flight on the caller's stream
+    if (!p->hyb_tabs) SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_tabs), tensor_rows_tab_bytes(p)));
+    if (!p->hyb_g) SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_g), tensor_rows_g_bytes(p)));
+    if (!p->hyb_s1) {
+      // FP16 column spectra: 2 parts x M x M halves per work tile the scratch holds
+      const size_t bytes = (size_t)p->chunk * 2 * p->M * p->M * sizeof(__half);
+      SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_s1), bytes));
+      p->hyb_s1_bytes = bytes;
+    }
+    p->schedule = sch;
+    SRK_TRY(refresh_direct(p, nullptr));
+    SRK_CUDA(cudaStreamSynchronize(nullptr));
+    return SRK_OK;
+  }
   if (sch == SRK_SCHEDULE_DIRECT) {
     std::string why;
     if (!direct_supported(p, p->N, &why)) return fail(SRK_ERR_UNSUPPORTED, "direct schedule: %s", why.c_str());
@@ -516,6 +543,7 @@ srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
   }
   p->schedule = sch;
   p->direct_ready = false;
+  p->hyb_ready = false;
   return SRK_OK;
 }
 
@@ -1395,6 +1423,30 @@ srk_status srk_autotune(int N, int W, int erosion, float dx, int B, srk_dtype dt
         if (st == SRK_OK && ms < best) {
           best = ms;
           bestS = SRK_SCHEDULE_DIRECT;
+        }
+      }
+      srk_plan_destroy(p);
+      if (st != SRK_OK) return done(st);
+    }
+  }
+  if (dtype != SRK_F32 && 512 - 2 * erosion >= 16) {
+    // the tensor-core row pass (tile 512), where it applies
+    srk_plan p = nullptr;
+    if (srk_plan_create(&p, N, W, erosion, dx, Bt, N + (N & 1), dtype, 512, 0) == SRK_OK) {
+      std::string why;
+      if (tensor_rows_supported(p, &why) && srk_plan_set_schedule(p, SRK_SCHEDULE_TENSOR_ROWS) == SRK_OK &&
+          (st = srk_plan_set_kernel(p, Kx, Ky, KW, s)) == SRK_OK) {
+        for (int it = 0; it < 2; ++it) op_forward(E, E, Bt, s, R, p);
+        cudaEventRecord(e0, s);
+        for (int it = 0; it < 3; ++it) op_forward(E, E, Bt, s, R, p);
+        cudaEventRecord(e1, s);
+        st = srk_plan_sync(p, s);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (st == SRK_OK && ms < best) {
+          best = ms;
+          bestM = 512;
+          bestS = SRK_SCHEDULE_TENSOR_ROWS;
         }
       }
       srk_plan_destroy(p);
