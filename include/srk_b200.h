@@ -124,7 +124,11 @@ const char* srk_last_error(void);
  *         (cached on disk, see srk_autotune), else 128, 256 or 512.
  * scratch_budget_bytes: 0 = default (8 GiB, at most 1/16 of the device
  *         memory, at least 256 MiB); the scratch holds the work tiles in
- *         flight (5.8 MB each at N = 512), never more than B_max needs. */
+ *         flight (5.8 MB each at N = 512), never more than B_max needs.
+ * The plan also holds 2 W^2 B_max floats for the intermediate of the VJP
+ * and the tangent-adjoint (u*v between the FFT passes and the transposed
+ * stencil): every device buffer an operator uses is allocated here (plus the
+ * ragged / slab tile tables on a key's first call), none by an operator. */
 srk_status srk_plan_create(srk_plan* plan, int N, int W, int erosion, float dx, int B_max, int spectra_M,
                            srk_dtype dtype, int tile_M, size_t scratch_budget_bytes);
 srk_status srk_plan_destroy(srk_plan plan);

@@ -92,14 +92,14 @@ srk_status launch_conv_dt(srk_plan_s* p, const OpArgs& a, const Geom& g, bool co
   return fail(SRK_ERR_UNSUPPORTED, "dtype %d", (int)p->dtype);
 }
 
-srk_status ensure_wbuf(srk_plan_s* p, size_t bytes, cudaStream_t s) {
+// The W-sized intermediate of the VJP and the tangent-adjoint (wx, wy = u*v
+// between the engine's P3 and the transposed stencil) lives in a buffer the
+// plan allocates at creation (2 W^2 B_max floats): no operator allocates.
+srk_status ensure_wbuf(srk_plan_s* p, size_t bytes, cudaStream_t) {
   if (p->wbuf_bytes >= bytes) return SRK_OK;
-  if (p->wbuf) SRK_CUDA(cudaFreeAsync(p->wbuf, s));
-  p->wbuf = nullptr;
-  p->wbuf_bytes = 0;
-  SRK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p->wbuf), bytes, s));
-  p->wbuf_bytes = bytes;
-  return SRK_OK;
+  return fail(SRK_ERR_UNSUPPORTED,
+              "the call needs %zu bytes of derivative intermediate, the plan holds %zu (2 W^2 B_max floats)", bytes,
+              p->wbuf_bytes);
 }
 
 template <typename T>
@@ -406,6 +406,12 @@ srk_status srk_plan_create(srk_plan* out, int N, int W, int erosion, float dx, i
       return cleanup(cuda_status(err, "spectrum allocation"));
   if ((err = cudaMalloc(reinterpret_cast<void**>(&p->tw), sizeof(float2) * M)) != cudaSuccess)
     return cleanup(cuda_status(err, "twiddle allocation"));
+  // the derivative operators' intermediate (ensure_wbuf), allocated here once
+  p->wbuf_bytes = 2 * (size_t)W * W * (size_t)B_max * sizeof(float);
+  if ((err = cudaMalloc(reinterpret_cast<void**>(&p->wbuf), p->wbuf_bytes)) != cudaSuccess) {
+    p->wbuf_bytes = 0;
+    return cleanup(cuda_status(err, "derivative intermediate allocation"));
+  }
   if ((err = cudaMalloc(reinterpret_cast<void**>(&p->ctl), sizeof(Ctl))) != cudaSuccess)
     return cleanup(cuda_status(err, "control block allocation"));
   if ((err = cudaHostAlloc(reinterpret_cast<void**>(&p->mailbox), 2 * sizeof(unsigned int), cudaHostAllocDefault)) !=
