@@ -30,7 +30,9 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
   auto launch3 = [&](int w0, int c, float2* base, __half* planes, cudaStream_t s1s, cudaStream_t s2s,
                      cudaStream_t s3s, cudaEvent_t e1, cudaEvent_t e2) -> srk_status {
-    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, s1s>>>(a, g, p->tw, w0, planes, c, p->nsm);
+    CUtensorMap pmap;
+    SRK_TRY(tensor_rows_plane_map(planes, c, kP1hCols, 1, kP1hBox, &pmap));
+    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, s1s>>>(pmap, a, g, p->tw, w0, p->nsm);
     if (e1) {
       SRK_CUDA(cudaEventRecord(e1, s1s));
       SRK_CUDA(cudaStreamWaitEvent(s2s, e1, 0));

@@ -21,9 +21,9 @@
 //   KT/8 + 16 slots x 128 bytes per (ky, field, part), read through a
 //   descriptor with leading = stride byte offset = 128 (direct.cu explains the
 //   identity).  Tables scaled by a power of two (max |g| in [8, 16)).
-// * Accumulators: 4 x 64 TMEM columns (Gx re/im, Gy re/im); two CTAs per
-//   SM, so one CTA's epilogue (its S2 stores) overlaps the other's loads
-//   and MMAs.
+// * Persistent, one CTA per SM: two shared-memory stages and two sets of
+//   4 x 64 TMEM accumulator columns (Gx re/im, Gy re/im), so the epilogue of
+//   one item (its S2 stores) overlaps the loads and MMAs of the next.
 // * Precision: FP16 operands (Z and g rounded once), FP32 accumulation — for
 //   the FP16/BF16 storage forms (rel 1e-2 / abs 1e-3).
 #include <cuda.h>
@@ -55,63 +55,106 @@ struct Args {
   int c, e, S, P;         // work tiles in the chunk, erosion, valid stride, S2 pitch
 };
 
-__host__ __device__ inline size_t smem_bytes(int e) {
+__host__ __device__ inline size_t stage_bytes(int e) {
   const size_t bpart = (size_t)(kt_of(e) / 8) * NB * 16;
-  return 1024 + 2 * bpart + 4 * (size_t)qs_of(e) * 128;
+  return 2 * bpart + 4 * (size_t)qs_of(e) * 128;
+}
+__host__ __device__ inline size_t smem_bytes(int e) { return 1024 + 2 * stage_bytes(e); }
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 
-__global__ void __launch_bounds__(kThreadsH, 2) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
+// Persistent: one CTA per SM walks the items (x'-tile j, ky, batch of NB work
+// tiles) with a stride of the grid.  Two shared-memory stages (B planes + A
+// bands) and two TMEM accumulator sets let the loads of item k+1 and the
+// MMAs of item k+1 run while the epilogue of item k drains its accumulators.
+//   full[s]  : stage s loaded (TMA / bulk copy bytes)     empty[s] : stage s read by the MMAs (commit)
+//   tfull[t] : accumulators t complete (commit)           tempty[t]: accumulators t drained (4 epilogue warps)
+__global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int e = a.e, KT = kt_of(e), KC = KT / 8, QS = qs_of(e);
   const uint32_t lboB = (uint32_t)NB * 16;      // bytes between 8-column chunks of B
   const uint32_t bpart = (uint32_t)KC * lboB;   // one part (re / im) of the B tile
   const uint32_t tab = (uint32_t)QS * 128;      // one (field, part) band
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* accfull = full + 1;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accfull + 1);
-  unsigned char* Bs = smem + 1024;
-  unsigned char* As = Bs + 2 * bpart;
+  const uint32_t stage = 2 * bpart + 4 * tab;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // [2]
+  uint64_t* empty = full + 2;                          // [2]
+  uint64_t* tfull = empty + 2;                         // [2]
+  uint64_t* tempty = tfull + 2;                        // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  unsigned char* St = smem + 1024;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int j = blockIdx.x, ky = blockIdx.y;
-  const int xk0 = MT * j;          // first input column of the tile's band
-  const int wl0 = NB * blockIdx.z; // first work tile of the batch
+  const int ntx = (a.S + MT - 1) / MT, nbatch = (a.c + NB - 1) / NB;
+  const int items = ntx * M * nbatch;
   const unsigned long long lim = a.spin_limit;
 
   if (threadIdx.x == 0) {
-    mbar_init(full, 1);
-    mbar_init(accfull, 1);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(full + i, 1);
+      mbar_init(empty + i, 1);
+      mbar_init(tfull + i, 1);
+      mbar_init(tempty + i, 4);
+    }
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(4 * NB));
+                 "r"(8 * NB));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  auto decode = [&](int item, int& j, int& ky, int& batch) {
+    j = item % ntx;
+    const int r = item / ntx;
+    ky = r % M;
+    batch = r / M;
+  };
 
   if (warp == 4) {
     if (lane == 0) {
-      mbar_expect_tx(full, 2 * bpart + 4 * tab);
-      for (int part = 0; part < 2; ++part)
-        for (int cc = 0; cc < KC; ++cc)
-          tma_load_3d(Bs + part * bpart + cc * lboB, &zmap, xk0 + 8 * cc, wl0, ky * 2 + part, full);
-      bulk_g2s(As, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, full);
+      int issued = 0;
+      for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
+        const int s = k & 1;
+        if (k >= 2 && !mbar_wait(empty + s, (unsigned)((k / 2 - 1) & 1), lim)) {
+          atomicCAS(a.err, 0u, 13u);
+          *abort_flag = 1;
+        }
+        if (*abort_flag) break;
+        int j, ky, batch;
+        decode(item, j, ky, batch);
+        unsigned char* Bs = St + (size_t)s * stage;
+        mbar_expect_tx(full + s, stage);
+        for (int part = 0; part < 2; ++part)
+          for (int cc = 0; cc < KC; ++cc)
+            tma_load_3d(Bs + part * bpart + cc * lboB, &zmap, MT * j + 8 * cc, NB * batch, ky * 2 + part, full + s);
+        bulk_g2s(Bs + 2 * bpart, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, full + s);
+        ++issued;
+      }
       // every copy has landed before the CTA can leave (also on the error path)
-      mbar_wait(full, 0, lim);
+      for (int k = issued > 2 ? issued - 2 : 0; k < issued; ++k) mbar_wait(full + (k & 1), (unsigned)((k / 2) & 1), lim);
     }
     __syncwarp();
   } else if (warp == 5) {
     if (lane == 0) {
       const uint32_t id = idesc_f16(0, MT, NB);
       const uint32_t idn = id | (1u << 13);  // negate A
-      if (!mbar_wait(full, 0, lim)) {
-        atomicCAS(a.err, 0u, 11u);
-      } else {
+      for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
+        const int s = k & 1, t = k & 1;
+        if (!mbar_wait(full + s, (unsigned)((k / 2) & 1), lim) ||
+            (k >= 2 && !mbar_wait(tempty + t, (unsigned)((k / 2 - 1) & 1), lim))) {
+          atomicCAS(a.err, 0u, 11u);
+          *abort_flag = 1;
+        }
+        if (*abort_flag) break;
         tc_fence_after();
-        const uint32_t b0 = smem_u32(Bs), a0 = smem_u32(As);
+        const uint32_t b0 = smem_u32(St + (size_t)s * stage), a0 = b0 + 2 * bpart;
+        const uint32_t d0 = tmem + (uint32_t)t * 4 * NB;
         for (int ks = 0; ks < KT / 16; ++ks) {
           const uint64_t dbr = sdesc(b0 + (uint32_t)ks * 2 * lboB, lboB, 128);
           const uint64_t dbi = sdesc(b0 + bpart + (uint32_t)ks * 2 * lboB, lboB, 128);
@@ -119,54 +162,70 @@ __global__ void __launch_bounds__(kThreadsH, 2) k_p2h(const __grid_constant__ CU
           for (int f = 0; f < 2; ++f) {
             const uint64_t dar = sdesc(a0 + (uint32_t)(f * 2 + 0) * tab + (uint32_t)ks * 256, 128, 128);
             const uint64_t dai = sdesc(a0 + (uint32_t)(f * 2 + 1) * tab + (uint32_t)ks * 256, 128, 128);
-            const uint32_t dr = tmem + (uint32_t)(f * 2 + 0) * NB, di = tmem + (uint32_t)(f * 2 + 1) * NB;
+            const uint32_t dr = d0 + (uint32_t)(f * 2 + 0) * NB, di = d0 + (uint32_t)(f * 2 + 1) * NB;
             mma_f16(dr, dar, dbr, id, ks > 0);   // + Tr Zr
             mma_f16(dr, dai, dbi, idn, true);    // - Ti Zi
             mma_f16(di, dar, dbi, id, ks > 0);   // + Tr Zi
             mma_f16(di, dai, dbr, id, true);     // + Ti Zr
           }
         }
+        mma_commit(empty + s);  // stage s free once these MMAs have read it
+        mma_commit(tfull + t);  // accumulators t complete
       }
-      mma_commit(accfull);
     }
     __syncwarp();
   } else {
-    bool ok = true;
-    if (lane == 0) ok = mbar_wait(accfull, 0, lim);
-    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-    if (!ok && lane == 0) atomicCAS(a.err, 0u, 12u);
-    if (ok) {
+    const int mrow = warp * 32 + lane;            // TMEM lane (rows reversed)
+    const float sc = ldexpf(1.f, -__ldg(a.tab_exp));
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const size_t fo = (size_t)a.P * M;            // S2 field stride
+    for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
+      const int t = k & 1;
+      bool ok = true;
+      if (lane == 0) ok = mbar_wait(tfull + t, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) {
+        if (lane == 0) {
+          atomicCAS(a.err, 0u, 12u);
+          *abort_flag = 1;
+        }
+        break;
+      }
       tc_fence_after();
-      const int mrow = warp * 32 + lane;            // TMEM lane (rows reversed)
-      const int xv = MT * j + MT - 1 - mrow;        // valid-column index x' - e
-      const float sc = ldexpf(1.f, -__ldg(a.tab_exp));
-      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-      const size_t fo = (size_t)a.P * M;            // S2 field stride
+      int j, ky, batch;
+      decode(item, j, ky, batch);
+      const int xv = MT * j + MT - 1 - mrow;      // valid-column index x' - e
+      const int wl0 = NB * batch;
       const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)ky * 4 + (xv & 3);
+      const uint32_t tb = trow + (uint32_t)t * 4 * NB;
       for (int n0 = 0; n0 < NB; n0 += 16) {
         float r0[16], i0[16], r1[16], i1[16];
-        tmem_ld16(trow + 0 * NB + (uint32_t)n0, r0);
-        tmem_ld16(trow + 1 * NB + (uint32_t)n0, i0);
-        tmem_ld16(trow + 2 * NB + (uint32_t)n0, r1);
-        tmem_ld16(trow + 3 * NB + (uint32_t)n0, i1);
+        tmem_ld16(tb + 0 * NB + (uint32_t)n0, r0);
+        tmem_ld16(tb + 1 * NB + (uint32_t)n0, i0);
+        tmem_ld16(tb + 2 * NB + (uint32_t)n0, r1);
+        tmem_ld16(tb + 3 * NB + (uint32_t)n0, i1);
         tmem_wait_ld();
         if (xv >= a.S) continue;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          const int wl = wl0 + n0 + k;
+        for (int q = 0; q < 16; ++q) {
+          const int wl = wl0 + n0 + q;
           if (wl >= a.c) break;
           float2* s2 = a.scratch + (size_t)wl * a.per + a.s1 + xo;
-          __stcg(s2, make_float2(r0[k] * sc, i0[k] * sc));
-          __stcg(s2 + fo, make_float2(r1[k] * sc, i1[k] * sc));
+          __stcg(s2, make_float2(r0[q] * sc, i0[q] * sc));
+          __stcg(s2 + fo, make_float2(r1[q] * sc, i1[q] * sc));
         }
       }
+      // the accumulators t are free for item k + 2
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty + t);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 5) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * NB));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(8 * NB));
   }
 }
 
@@ -276,22 +335,27 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn_h() {
 }
 }  // namespace
 
+srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
+                                 CUtensorMap* out) {
+  auto enc = encode_fn_h();
+  if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+  std::memset(out, 0, sizeof(*out));
+  const cuuint64_t dims[3] = {(cuuint64_t)hyb::M, (cuuint64_t)c, (cuuint64_t)(2 * hyb::M)};
+  const cuuint64_t strides[2] = {(cuuint64_t)hyb::M * 2, (cuuint64_t)c * hyb::M * 2};
+  const cuuint32_t box[3] = {box_x, box_w, box_p};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<__half*>(planes), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SRK_OK : fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+}
+
 // The row pass of one chunk of c work tiles: planes [2M][c][M] FP16 (k_p1h)
 // -> S2 of every work tile at scratch + wl*per + s1 (P3's layout).
 srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
                           int P, cudaStream_t s) {
-  auto enc = encode_fn_h();
-  if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
   CUtensorMap map;
-  std::memset(&map, 0, sizeof(map));
-  const cuuint64_t dims[3] = {(cuuint64_t)hyb::M, (cuuint64_t)c, (cuuint64_t)(2 * hyb::M)};
-  const cuuint64_t strides[2] = {(cuuint64_t)hyb::M * 2, (cuuint64_t)c * hyb::M * 2};
-  const cuuint32_t box[3] = {8, (cuuint32_t)hyb::NB, 1};
-  const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<__half*>(planes), dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  SRK_TRY(tensor_rows_plane_map(planes, c, 8, hyb::NB, 1, &map));
   hyb::Args a;
   a.tabs = p->hyb_tabs;
   a.tab_exp = reinterpret_cast<const int*>(p->direct_err + 2);
@@ -306,7 +370,8 @@ srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* sc
   a.P = P;
   const size_t sm = hyb::smem_bytes(p->e);
   SRK_CUDA(cudaFuncSetAttribute(hyb::k_p2h, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const dim3 grid((S + hyb::MT - 1) / hyb::MT, hyb::M, (c + hyb::NB - 1) / hyb::NB);
+  const long long items = (long long)((S + hyb::MT - 1) / hyb::MT) * hyb::M * ((c + hyb::NB - 1) / hyb::NB);
+  const int grid = (int)std::min<long long>(items, p->nsm > 0 ? p->nsm : 148);
   hyb::k_p2h<<<grid, hyb::kThreadsH, sm, s>>>(map, a);
   return cuda_status(cudaGetLastError(), "tensor-row pass launch");
 }

@@ -4,12 +4,16 @@
 // in the layout the tensor-core row pass (hybrid.cu) reads with TMA:
 //   planes[((ky * 2 + part) * c + wl) * M + x]      (part 0 = re, 1 = im),
 // c = work tiles in the chunk, wl = work tile within the chunk.  Each CTA
-// transforms 8 consecutive columns (two units of four) and writes, for every
-// (ky, part), their 8 values as one 16-byte store.  Only for single-field
+// transforms 8 consecutive columns (two units of four), stages their values
+// [ky][part][8] in shared memory and writes them with TMA stores (one
+// 16-byte piece per (ky, part) plane row).  Only for single-field
 // ops (one complex field per work tile: OP_FWD, OP_VJP_F, OP_JVP,
 // OP_TANADJ_F).
 #pragma once
+#include <cuda.h>
+
 #include "engine.cuh"
+#include "tc.cuh"
 
 namespace srk {
 
@@ -21,13 +25,17 @@ constexpr int kHybM = 512;
 // (whole 32-byte sectors, but 3 CTAs per SM and twice the transforms per
 // line).
 constexpr int kP1hCols = 8;
+// Byte offset of the staging block (128-byte aligned: the source of TMA stores).
+__host__ __device__ constexpr size_t p1h_stage_offset() { return (phase_smem_bytes<kHybM>() + 127) / 128 * 128; }
 __host__ __device__ constexpr size_t p1h_smem_bytes() {
-  return phase_smem_bytes<kHybM>() + (size_t)kHybM * 2 * kP1hCols * sizeof(__half);
+  return p1h_stage_offset() + (size_t)kHybM * 2 * kP1hCols * sizeof(__half);
 }
+// Planes written per TMA store (box {8 columns, 1 work tile, kP1hBox planes}).
+constexpr int kP1hBox = 256;
 
 template <int OP, typename T>
 __global__ void __launch_bounds__(kThreads, SRK_P1_MIN_BLOCKS)
-k_p1h(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, __half* __restrict__ planes, int c, int ahead) {
+k_p1h(const __grid_constant__ CUtensorMap pmap, OpArgs a, Geom g, const float2* __restrict__ twg, int w0, int ahead) {
   constexpr int M = kHybM;
   constexpr int TPF = tpf_of<M>();
   constexpr int EPT = M / TPF;
@@ -39,7 +47,7 @@ k_p1h(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, __half* __restri
   load_twiddles(sm, twg, M);
   __syncthreads();
   float2* rows = sm + tw_slots<M>();
-  __half* st = reinterpret_cast<__half*>(rows + 2 * LPU * row_stride<M>());  // [ky][part][kP1hCols columns]
+  __half* st = reinterpret_cast<__half*>(reinterpret_cast<unsigned char*>(sm) + p1h_stage_offset());  // [ky][part][8]
   const int wl = blockIdx.y, w = w0 + wl;
   const int xb = blockIdx.x;  // columns kP1hCols * xb ..
   if (ahead > 0) {
@@ -65,13 +73,15 @@ k_p1h(OpArgs a, Geom g, const float2* __restrict__ twg, int w0, __half* __restri
 #pragma unroll
     for (int i = 0; i < EPT; ++i) za[i] = zb[i];
   }
+  // the staging block [plane = 2 ky + part][8 columns] is the layout of the
+  // store box {8 columns, 1 work tile, kP1hBox planes}: the TMA engine writes
+  // the 1024 16-byte row pieces (the threads would need 1024 scattered stores)
+  tc::fence_async_smem();
   __syncthreads();
-  const size_t x0 = (size_t)xb * kP1hCols;
-  constexpr int PIECES = kP1hCols / 8;  // 16-byte pieces per (ky, part)
-  for (int j = threadIdx.x; j < M * 2 * PIECES; j += kThreads) {
-    const int plane = j / PIECES, piece = j % PIECES;
-    __stcg(reinterpret_cast<uint4*>(planes + ((size_t)plane * c + wl) * M + x0 + 8 * piece),
-           *reinterpret_cast<const uint4*>(st + plane * kP1hCols + 8 * piece));
+  if (threadIdx.x == 0) {
+    for (int p0 = 0; p0 < 2 * M; p0 += kP1hBox) tc::tma_store_3d(&pmap, xb * kP1hCols, wl, p0, st + p0 * kP1hCols);
+    tc::bulk_commit();
+    tc::bulk_wait_all();
   }
 }
 

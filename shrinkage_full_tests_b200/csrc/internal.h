@@ -3,6 +3,7 @@
 // explicit instantiation per storage type lives in conv_<type>.cu so the
 // kernel families compile in parallel).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
@@ -162,6 +163,9 @@ size_t tensor_rows_g_bytes(const srk_plan_s* p);
 srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s);
 srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
                           int P, cudaStream_t s);
+// Tensor map of a chunk's FP16 planes [2M][c][M] with the given box.
+srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
+                                 CUtensorMap* out);
 
 // Spectrum kernels defined in spectra.cuh (compiled once, in srk_abi.cu) and
 // launched from the other translation units too.
