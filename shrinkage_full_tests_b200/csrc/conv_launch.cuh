@@ -28,49 +28,53 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   const size_t sm3 = phase_smem_bytes<M>() + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
   SRK_TRY(set_smem(k_p1h<OP, T>, smp1));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
-  auto launch3 = [&](int w0, int c, float2* base, __half* planes, cudaStream_t s1s, cudaStream_t s2s,
-                     cudaStream_t s3s, cudaEvent_t e1, cudaEvent_t e2) -> srk_status {
+  auto p1 = [&](int w0, int c, __half* planes, cudaStream_t st) -> srk_status {
     CUtensorMap pmap;
     SRK_TRY(tensor_rows_plane_map(planes, c, kP1hCols, 1, kP1hBox, &pmap));
-    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, s1s>>>(pmap, a, g, p->tw, w0, p->nsm);
-    if (e1) {
-      SRK_CUDA(cudaEventRecord(e1, s1s));
-      SRK_CUDA(cudaStreamWaitEvent(s2s, e1, 0));
-    }
-    SRK_TRY(tensor_rows_p2(p, planes, c, base, per, s1, g.S, s2_pitch(g.S), s2s));
-    if (e2) {
-      SRK_CUDA(cudaEventRecord(e2, s2s));
-      SRK_CUDA(cudaStreamWaitEvent(s3s, e2, 0));
-    }
-    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, s3s>>>(base, a, g, p->tw, w0, p->nsm);
+    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, p->nsm);
     return SRK_OK;
+  };
+  auto p3 = [&](int w0, int c, float2* base, cudaStream_t st) {
+    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, st>>>(base, a, g, p->tw, w0, p->nsm);
   };
   const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
   int launches = 0;
-  constexpr int R = srk_plan_s::kRing;
-  if (nwt <= whole || !p->overlap || !p->ps1 || cap < (size_t)R) {
-    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 3)
-      SRK_TRY(launch3(w0, std::min(whole, nwt - w0), p->scratch, p->hyb_s1, s, s, s, nullptr, nullptr));
+  if (nwt < 256 || !p->overlap || !p->ps1 || cap < 2) {
+    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 3) {
+      const int c = std::min(whole, nwt - w0);
+      SRK_TRY(p1(w0, c, p->hyb_s1, s));
+      SRK_TRY(tensor_rows_p2(p, p->hyb_s1, c, p->scratch, per, s1, g.S, s2_pitch(g.S), s));
+      p3(w0, c, p->scratch, s);
+    }
   } else {
-    // the ring of launch_conv_m (P1h of chunk k after the row pass of chunk
-    // k-R has read its planes; the row pass after P3 of chunk k-R has read
-    // the slot's S2)
-    const int chunk = (int)std::min<size_t>(cap / R, 65535);
+    // Two slots of chunks.  The persistent row pass occupies every SM, so it
+    // runs alone: P2h(k) (caller's stream) waits for P1h(k) and follows
+    // P3(k-1) in stream order; P1h(k+1) (plan stream) starts after P2h(k) and
+    // runs beside P3(k).  Slot reuse: P1h(k+1) rewrites the planes P2h(k-1)
+    // read (it waits for P2h(k)); P2h(k) rewrites the S2 P3(k-2) read
+    // (earlier on the same stream).
+    // at least four chunks where the slots allow (the overlap is between chunks)
+    const int chunk = (int)std::min<size_t>({cap / 2, (size_t)std::max(128, (nwt + 3) / 4), (size_t)65535});
+    const int nch = (nwt + chunk - 1) / chunk;
+    auto planes_of = [&](int k) { return p->hyb_s1 + (size_t)(k & 1) * chunk * plane_wt; };
+    auto base_of = [&](int k) { return p->scratch + (size_t)(k & 1) * chunk * per; };
+    auto count_of = [&](int k) { return std::min(chunk, nwt - k * chunk); };
     SRK_CUDA(cudaEventRecord(p->ev_fork, s));
     SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev_fork, 0));
-    SRK_CUDA(cudaStreamWaitEvent(p->ps3, p->ev_fork, 0));
-    int k = 0;
-    for (int w0 = 0; w0 < nwt; w0 += chunk, ++k, launches += 3) {
-      const int r = k % R;
-      if (k >= R) {
-        SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev2[r], 0));
-        SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[r], 0));
+    SRK_TRY(p1(0, count_of(0), planes_of(0), p->ps1));
+    SRK_CUDA(cudaEventRecord(p->ev1[0], p->ps1));
+    for (int k = 0; k < nch; ++k, launches += 3) {
+      SRK_CUDA(cudaStreamWaitEvent(s, p->ev1[k & 1], 0));
+      SRK_TRY(tensor_rows_p2(p, planes_of(k), count_of(k), base_of(k), per, s1, g.S, s2_pitch(g.S), s));
+      if (k + 1 < nch) {
+        SRK_CUDA(cudaEventRecord(p->ev2[k & 1], s));
+        SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev2[k & 1], 0));
+        SRK_TRY(p1((k + 1) * chunk, count_of(k + 1), planes_of(k + 1), p->ps1));
+        SRK_CUDA(cudaEventRecord(p->ev1[(k + 1) & 1], p->ps1));
       }
-      SRK_TRY(launch3(w0, std::min(chunk, nwt - w0), p->scratch + r * (size_t)chunk * per,
-                      p->hyb_s1 + r * (size_t)chunk * plane_wt, p->ps1, s, p->ps3, p->ev1[r], p->ev2[r]));
-      SRK_CUDA(cudaEventRecord(p->ev3[r], p->ps3));
+      p3(k * chunk, count_of(k), base_of(k), s);
     }
-    SRK_CUDA(cudaStreamWaitEvent(s, p->ev3[(k - 1) % R], 0));
+    // every plan-stream launch is followed by a row pass on the caller's stream: joined
   }
   p->last_launches = launches;
   return cuda_status(cudaGetLastError(), "tensor-row launch");

@@ -39,7 +39,9 @@ using namespace srk::tc;
 constexpr int M = 512;
 constexpr int MT = 128;        // outputs x' per tile = TMEM lanes
 constexpr int NB = 64;         // work tiles per MMA (N): 2 CTAs per SM (4 x 64 TMEM columns each)
-constexpr int kThreadsH = 192;
+constexpr int kEpiWarps = 4;                      // one warp per TMEM lane quarter (8 measured no faster)
+constexpr int kThreadsH = 32 * (kEpiWarps + 2);    // + the load warp and the MMA warp
+constexpr int kLoadWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr int kMaxE = 64;
 
 __host__ __device__ constexpr int kt_of(int e) { return ((MT + 2 * e) + 15) / 16 * 16; }  // input columns per tile
@@ -70,7 +72,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 // bands) and two TMEM accumulator sets let the loads of item k+1 and the
 // MMAs of item k+1 run while the epilogue of item k drains its accumulators.
 //   full[s]  : stage s loaded (TMA / bulk copy bytes)     empty[s] : stage s read by the MMAs (commit)
-//   tfull[t] : accumulators t complete (commit)           tempty[t]: accumulators t drained (4 epilogue warps)
+//   tfull[t] : accumulators t complete (commit)           tempty[t]: accumulators t drained (every epilogue warp)
 __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int e = a.e, KT = kt_of(e), KC = KT / 8, QS = qs_of(e);
@@ -95,12 +97,12 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
       mbar_init(full + i, 1);
       mbar_init(empty + i, 1);
       mbar_init(tfull + i, 1);
-      mbar_init(tempty + i, 4);
+      mbar_init(tempty + i, kEpiWarps);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(8 * NB));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
     batch = r / M;
   };
 
-  if (warp == 4) {
+  if (warp == kLoadWarp) {
     if (lane == 0) {
       int issued = 0;
       for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
       for (int k = issued > 2 ? issued - 2 : 0; k < issued; ++k) mbar_wait(full + (k & 1), (unsigned)((k / 2) & 1), lim);
     }
     __syncwarp();
-  } else if (warp == 5) {
+  } else if (warp == kMmaWarp) {
     if (lane == 0) {
       const uint32_t id = idesc_f16(0, MT, NB);
       const uint32_t idn = id | (1u << 13);  // negate A
@@ -175,9 +177,12 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
     }
     __syncwarp();
   } else {
-    const int mrow = warp * 32 + lane;            // TMEM lane (rows reversed)
+    // epilogue warp: TMEM lane quarter (warp % 4) and its share of the NB columns
+    constexpr int kCols = NB / (kEpiWarps / 4);
+    const int quarter = warp & 3, colh = warp >> 2;
+    const int mrow = quarter * 32 + lane;         // TMEM lane (rows reversed)
     const float sc = ldexpf(1.f, -__ldg(a.tab_exp));
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
     const size_t fo = (size_t)a.P * M;            // S2 field stride
     for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
       const int t = k & 1;
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
       const int wl0 = NB * batch;
       const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)ky * 4 + (xv & 3);
       const uint32_t tb = trow + (uint32_t)t * 4 * NB;
-      for (int n0 = 0; n0 < NB; n0 += 16) {
+      for (int n0 = colh * kCols; n0 < (colh + 1) * kCols; n0 += 16) {
         float r0[16], i0[16], r1[16], i1[16];
         tmem_ld16(tb + 0 * NB + (uint32_t)n0, r0);
         tmem_ld16(tb + 1 * NB + (uint32_t)n0, i0);
@@ -223,7 +228,7 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(8 * NB));
   }
