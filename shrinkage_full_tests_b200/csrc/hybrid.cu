@@ -15,8 +15,9 @@
 //   D[m][n] = sum_k T[m][k] Z_n[ky][128 j + k],  T[m][k] = g[m - k + e],
 // complex: Ur = Tr Zr - Ti Zi, Ui = Tr Zi + Ti Zr, four real MMAs per K step
 // and field (the minus sign by the instruction descriptor's negate-A bit).
-// * B (Z planes, FP16, written by k_p1h) by TMA: box {8 columns x, 128 work
-//   tiles, 1 plane}, one box per 16-byte K chunk — the K-major operand.
+// * B (Z planes, FP16, written by k_p1h) by TMA with the 128-byte swizzle:
+//   box {64 columns x, 64 work tiles, 1 plane}, the K-major SWIZZLE_128B
+//   operand (4 boxes per part at e = 60).
 // * A (the band T) never materialised: rows reversed, one slot table of
 //   KT/8 + 16 slots x 128 bytes per (ky, field, part), read through a
 //   descriptor with leading = stride byte offset = 128 (direct.cu explains the
@@ -44,7 +45,8 @@ constexpr int kThreadsH = 32 * (kEpiWarps + 2);    // + the load warp and the MM
 constexpr int kLoadWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr int kMaxE = 64;
 
-__host__ __device__ constexpr int kt_of(int e) { return ((MT + 2 * e) + 15) / 16 * 16; }  // input columns per tile
+// input columns per tile, a whole number of 64-column (128-byte) swizzle atoms
+__host__ __device__ constexpr int kt_of(int e) { return ((MT + 2 * e) + 63) / 64 * 64; }
 __host__ __device__ constexpr int qs_of(int e) { return kt_of(e) / 8 + MT / 8; }           // band slots
 
 struct Args {
@@ -58,7 +60,7 @@ struct Args {
 };
 
 __host__ __device__ inline size_t stage_bytes(int e) {
-  const size_t bpart = (size_t)(kt_of(e) / 8) * NB * 16;
+  const size_t bpart = (size_t)kt_of(e) * NB * 2;
   return 2 * bpart + 4 * (size_t)qs_of(e) * 128;
 }
 __host__ __device__ inline size_t smem_bytes(int e) { return 1024 + 2 * stage_bytes(e); }
@@ -75,9 +77,12 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
 //   tfull[t] : accumulators t complete (commit)           tempty[t]: accumulators t drained (every epilogue warp)
 __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  const int e = a.e, KT = kt_of(e), KC = KT / 8, QS = qs_of(e);
-  const uint32_t lboB = (uint32_t)NB * 16;      // bytes between 8-column chunks of B
-  const uint32_t bpart = (uint32_t)KC * lboB;   // one part (re / im) of the B tile
+  const int e = a.e, KT = kt_of(e), KB = KT / 64, QS = qs_of(e);
+  // B (one part): KB boxes of NB rows (work tiles) x 64 columns x (128 bytes,
+  // 128-byte swizzle) — the canonical K-major SWIZZLE_128B operand: 8-row
+  // groups 1024 bytes apart, K advanced by 32 bytes per MMA within an atom
+  const uint32_t boxB = (uint32_t)NB * 128;
+  const uint32_t bpart = (uint32_t)KB * boxB;
   const uint32_t tab = (uint32_t)QS * 128;      // one (field, part) band
   const uint32_t stage = 2 * bpart + 4 * tab;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // [2]
@@ -93,13 +98,15 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
   const unsigned long long lim = a.spin_limit;
 
   if (threadIdx.x == 0) {
+    // the swizzle atoms of the B boxes must sit on 1024-byte boundaries
+    *abort_flag = (smem_u32(St) & 1023u) != 0;
+    if (*abort_flag) atomicCAS(a.err, 0u, 14u);
     for (int i = 0; i < 2; ++i) {
       mbar_init(full + i, 1);
       mbar_init(empty + i, 1);
       mbar_init(tfull + i, 1);
       mbar_init(tempty + i, kEpiWarps);
     }
-    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == kMmaWarp) {
@@ -133,8 +140,8 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
         unsigned char* Bs = St + (size_t)s * stage;
         mbar_expect_tx(full + s, stage);
         for (int part = 0; part < 2; ++part)
-          for (int cc = 0; cc < KC; ++cc)
-            tma_load_3d(Bs + part * bpart + cc * lboB, &zmap, MT * j + 8 * cc, NB * batch, ky * 2 + part, full + s);
+          for (int kb = 0; kb < KB; ++kb)
+            tma_load_3d(Bs + part * bpart + kb * boxB, &zmap, MT * j + 64 * kb, NB * batch, ky * 2 + part, full + s);
         bulk_g2s(Bs + 2 * bpart, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, full + s);
         ++issued;
       }
@@ -158,8 +165,9 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
         const uint32_t b0 = smem_u32(St + (size_t)s * stage), a0 = b0 + 2 * bpart;
         const uint32_t d0 = tmem + (uint32_t)t * 4 * NB;
         for (int ks = 0; ks < KT / 16; ++ks) {
-          const uint64_t dbr = sdesc(b0 + (uint32_t)ks * 2 * lboB, lboB, 128);
-          const uint64_t dbi = sdesc(b0 + bpart + (uint32_t)ks * 2 * lboB, lboB, 128);
+          const uint32_t boff = (uint32_t)(ks >> 2) * boxB + (uint32_t)(ks & 3) * 32;
+          const uint64_t dbr = sdesc_sw128(b0 + boff);
+          const uint64_t dbi = sdesc_sw128(b0 + bpart + boff);
 #pragma unroll
           for (int f = 0; f < 2; ++f) {
             const uint64_t dar = sdesc(a0 + (uint32_t)(f * 2 + 0) * tab + (uint32_t)ks * 256, 128, 128);
@@ -341,7 +349,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn_h() {
 }  // namespace
 
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
-                                 CUtensorMap* out) {
+                                 CUtensorMap* out, bool swizzle128) {
   auto enc = encode_fn_h();
   if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
   std::memset(out, 0, sizeof(*out));
@@ -350,8 +358,9 @@ srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, un
   const cuuint32_t box[3] = {box_x, box_w, box_p};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 3, const_cast<__half*>(planes), dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                         CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? SRK_OK : fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
@@ -360,7 +369,7 @@ srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, un
 srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
                           int P, cudaStream_t s) {
   CUtensorMap map;
-  SRK_TRY(tensor_rows_plane_map(planes, c, 8, hyb::NB, 1, &map));
+  SRK_TRY(tensor_rows_plane_map(planes, c, 64, hyb::NB, 1, &map, true));
   hyb::Args a;
   a.tabs = p->hyb_tabs;
   a.tab_exp = reinterpret_cast<const int*>(p->direct_err + 2);

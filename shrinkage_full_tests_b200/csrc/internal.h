@@ -165,7 +165,7 @@ srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* sc
                           int P, cudaStream_t s);
 // Tensor map of a chunk's FP16 planes [2M][c][M] with the given box.
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
-                                 CUtensorMap* out);
+                                 CUtensorMap* out, bool swizzle128 = false);
 
 // Spectrum kernels defined in spectra.cuh (compiled once, in srk_abi.cu) and
 // launched from the other translation units too.

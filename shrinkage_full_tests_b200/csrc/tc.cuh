@@ -53,6 +53,13 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
   return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
+// The same for the K-major 128-byte-swizzle layout (rows of 64 16-bit
+// values, 8-row groups 1024 bytes apart; leading offset unused = 1): the
+// start address of an atom is 1024-byte aligned, plus the K offset.
+__device__ __forceinline__ uint64_t sdesc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
 // Instruction descriptor of kind::f16: FP32 accumulator, A/B format, both
 // K-major, N >> 3 at bit 17, M >> 4 at bit 24.
 __host__ __device__ constexpr uint32_t idesc_f16(int fmt, int M, int N) {
