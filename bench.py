@@ -418,8 +418,12 @@ def half_storage_rate(torch, srk, E32, GX, GY, N, W, e, dx, B, steps=20):
     ms = time_steps(torch, fn, steps, 3, None)
     peak, _ = measured_peaks()
     alg = B * (N * N + W * W) * 2
-    out = {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "dtype": "f16 storage, f32 arithmetic",
-           "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "tile_M": plan.info()["tile_M"]}
+    info = plan.info()
+    sched = ["persistent", "three_pass", "direct", "tensor_rows"][info["schedule"]]
+    arith = ("f32 FFTs, f16 x f16 -> f32 row convolution on the tensor cores" if sched == "tensor_rows"
+             else "f32 arithmetic")
+    out = {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "dtype": "f16 storage, " + arith,
+           "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "tile_M": info["tile_M"], "schedule": sched}
     del E, R, plan
     torch.cuda.empty_cache()
     return out

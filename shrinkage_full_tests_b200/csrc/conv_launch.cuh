@@ -14,8 +14,10 @@ srk_status set_smem(K kernel, size_t bytes) {
 }
 
 // Three-pass schedule with the tensor-core row pass (SRK_SCHEDULE_TENSOR_ROWS):
-// P1h (column FFT -> FP16 planes), the row pass of hybrid.cu (-> S2), P3
-// unchanged; the same ring of scratch slots and streams as launch_conv_m.
+// per chunk P1h (column FFT -> FP16 planes, with each work tile's largest
+// |Z|) and its refit pass (the work tiles outside FP16's comfortable range
+// again, scaled by a power of two), the row pass of hybrid.cu (-> S2), P3
+// unchanged; two slots of chunks on two streams.
 template <int OP, typename T>
 srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, cudaStream_t s) {
   constexpr int M = kHybM;
@@ -28,10 +30,18 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   const size_t sm3 = phase_smem_bytes<M>() + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
   SRK_TRY(set_smem(k_p1h<OP, T>, smp1));
   SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
-  auto p1 = [&](int w0, int c, __half* planes, cudaStream_t st) -> srk_status {
+  SRK_TRY(set_smem(k_p1h_refit<OP, T>, smp1));
+  int chunk = 0;  // work tiles per slot (two slots in the pipelined form)
+  // largest |Z| of the work tiles of the chunk in slot k & 1 (their planes' scales)
+  auto max_of = [&](int k) { return p->hyb_mx + (size_t)(k & 1) * chunk; };
+  auto p1 = [&](int k, int w0, int c, __half* planes, cudaStream_t st) -> srk_status {
     CUtensorMap pmap;
     SRK_TRY(tensor_rows_plane_map(planes, c, kP1hCols, 1, kP1hBox, &pmap));
-    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, p->nsm);
+    SRK_CUDA(cudaMemsetAsync(max_of(k), 0, (size_t)c * sizeof(unsigned int), st));
+    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, p->nsm, max_of(k),
+                                                                 p->direct_err);
+    k_p1h_refit<OP, T><<<std::max(p->nsm, 1) * 2, kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, c, max_of(k),
+                                                                        p->direct_err);
     return SRK_OK;
   };
   auto p3 = [&](int w0, int c, float2* base, cudaStream_t st) {
@@ -40,10 +50,10 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
   int launches = 0;
   if (nwt < 256 || !p->overlap || !p->ps1 || cap < 2) {
-    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 3) {
+    for (int w0 = 0; w0 < nwt; w0 += whole, launches += 4) {
       const int c = std::min(whole, nwt - w0);
-      SRK_TRY(p1(w0, c, p->hyb_s1, s));
-      SRK_TRY(tensor_rows_p2(p, p->hyb_s1, c, p->scratch, per, s1, g.S, s2_pitch(g.S), s));
+      SRK_TRY(p1(0, w0, c, p->hyb_s1, s));
+      SRK_TRY(tensor_rows_p2(p, p->hyb_s1, max_of(0), c, p->scratch, per, s1, g.S, s2_pitch(g.S), s));
       p3(w0, c, p->scratch, s);
     }
   } else {
@@ -54,22 +64,23 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
     // read (it waits for P2h(k)); P2h(k) rewrites the S2 P3(k-2) read
     // (earlier on the same stream).
     // at least four chunks where the slots allow (the overlap is between chunks)
-    const int chunk = (int)std::min<size_t>({cap / 2, (size_t)std::max(128, (nwt + 3) / 4), (size_t)65535});
+    chunk = (int)std::min<size_t>({cap / 2, (size_t)std::max(128, (nwt + 3) / 4), (size_t)65535});
     const int nch = (nwt + chunk - 1) / chunk;
     auto planes_of = [&](int k) { return p->hyb_s1 + (size_t)(k & 1) * chunk * plane_wt; };
     auto base_of = [&](int k) { return p->scratch + (size_t)(k & 1) * chunk * per; };
     auto count_of = [&](int k) { return std::min(chunk, nwt - k * chunk); };
     SRK_CUDA(cudaEventRecord(p->ev_fork, s));
     SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev_fork, 0));
-    SRK_TRY(p1(0, count_of(0), planes_of(0), p->ps1));
+    SRK_TRY(p1(0, 0, count_of(0), planes_of(0), p->ps1));
     SRK_CUDA(cudaEventRecord(p->ev1[0], p->ps1));
-    for (int k = 0; k < nch; ++k, launches += 3) {
+    for (int k = 0; k < nch; ++k, launches += 4) {
       SRK_CUDA(cudaStreamWaitEvent(s, p->ev1[k & 1], 0));
-      SRK_TRY(tensor_rows_p2(p, planes_of(k), count_of(k), base_of(k), per, s1, g.S, s2_pitch(g.S), s));
+      SRK_TRY(tensor_rows_p2(p, planes_of(k), max_of(k), count_of(k), base_of(k), per, s1, g.S, s2_pitch(g.S), s));
       if (k + 1 < nch) {
+        // the max words of slot (k+1) & 1 were last read by P2h(k-1), before P2h(k)
         SRK_CUDA(cudaEventRecord(p->ev2[k & 1], s));
         SRK_CUDA(cudaStreamWaitEvent(p->ps1, p->ev2[k & 1], 0));
-        SRK_TRY(p1((k + 1) * chunk, count_of(k + 1), planes_of(k + 1), p->ps1));
+        SRK_TRY(p1(k + 1, (k + 1) * chunk, count_of(k + 1), planes_of(k + 1), p->ps1));
         SRK_CUDA(cudaEventRecord(p->ev1[(k + 1) & 1], p->ps1));
       }
       p3(k * chunk, count_of(k), base_of(k), s);
@@ -85,8 +96,6 @@ srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt,
   if constexpr (M == kHybM && OpTraits<OP>::K == 1 && !std::is_same<T, float>::value) {
     if (p->schedule == SRK_SCHEDULE_TENSOR_ROWS && p->hyb_ready) return launch_tensor_rows<OP, T>(p, a, g, nwt, s);
   }
-  constexpr int K = OpTraits<OP>::K;
-  constexpr int L = OpTraits<OP>::L;
   const size_t sm1 = phase_smem_bytes<M>();
   const size_t sm2 = sm1 + p2_tile_bytes<M>(g.S);
   const size_t sm3 = sm1 + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);

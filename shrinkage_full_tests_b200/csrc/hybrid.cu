@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "hybrid_scale.cuh"
 #include "internal.h"
 #include "tc.cuh"
 
@@ -40,7 +41,11 @@ using namespace srk::tc;
 constexpr int M = 512;
 constexpr int MT = 128;        // outputs x' per tile = TMEM lanes
 constexpr int NB = 64;         // work tiles per MMA (N): 2 CTAs per SM (4 x 64 TMEM columns each)
-constexpr int kEpiWarps = 4;                      // one warp per TMEM lane quarter (8 measured no faster)
+#ifndef SRK_HYB_EPI_WARPS
+#define SRK_HYB_EPI_WARPS 4
+#endif
+constexpr int kEpiWarps = SRK_HYB_EPI_WARPS;      // a multiple of 4: each TMEM lane quarter split by columns
+static_assert(kEpiWarps >= 4 && kEpiWarps % 4 == 0 && kEpiWarps <= 16, "whole lane quarters, 16-column steps");
 constexpr int kThreadsH = 32 * (kEpiWarps + 2);    // + the load warp and the MMA warp
 constexpr int kLoadWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr int kMaxE = 64;
@@ -52,6 +57,7 @@ __host__ __device__ constexpr int qs_of(int e) { return kt_of(e) / 8 + MT / 8; }
 struct Args {
   const uint16_t* tabs;   // [M ky][2 field][2 part][QS][8][8] FP16 bits
   const int* tab_exp;     // tables hold g * 2^tab_exp
+  const unsigned int* mx; // largest |Z| per work tile (float bits): its planes hold Z * 2^plane_exp(mx[wl])
   float2* scratch;        // chunk base: S2 of work tile wl at scratch + wl*per + s1
   size_t per, s1;         // float2 per work tile, offset of S2 in it
   unsigned int* err;
@@ -189,11 +195,19 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
     constexpr int kCols = NB / (kEpiWarps / 4);
     const int quarter = warp & 3, colh = warp >> 2;
     const int mrow = quarter * 32 + lane;         // TMEM lane (rows reversed)
-    const float sc = ldexpf(1.f, -__ldg(a.tab_exp));
+    const int tab_exp = __ldg(a.tab_exp);
     const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
     const size_t fo = (size_t)a.P * M;            // S2 field stride
     for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
       const int t = k & 1;
+      int j, ky, batch;
+      decode(item, j, ky, batch);
+      const int wl0 = NB * batch;
+      // the largest |Z| words of the NB work tiles (columns lane, lane + 32),
+      // loaded before the wait for the accumulators so that their latency hides behind it
+      static_assert(NB == 64, "two column factors per lane");
+      const unsigned int z0 = __ldg(a.mx + min(wl0 + lane, a.c - 1));
+      const unsigned int z1 = __ldg(a.mx + min(wl0 + 32 + lane, a.c - 1));
       bool ok = true;
       if (lane == 0) ok = mbar_wait(tfull + t, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -205,12 +219,12 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
         break;
       }
       tc_fence_after();
-      int j, ky, batch;
-      decode(item, j, ky, batch);
       const int xv = MT * j + MT - 1 - mrow;      // valid-column index x' - e
-      const int wl0 = NB * batch;
       const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)ky * 4 + (xv & 3);
       const uint32_t tb = trow + (uint32_t)t * 4 * NB;
+      // the column factors 2^-(p + tab_exp)
+      const float sp0 = ldexpf(1.f, -plane_exp(z0) - tab_exp);
+      const float sp1 = ldexpf(1.f, -plane_exp(z1) - tab_exp);
       for (int n0 = colh * kCols; n0 < (colh + 1) * kCols; n0 += 16) {
         float r0[16], i0[16], r1[16], i1[16];
         tmem_ld16(tb + 0 * NB + (uint32_t)n0, r0);
@@ -218,14 +232,18 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
         tmem_ld16(tb + 2 * NB + (uint32_t)n0, r1);
         tmem_ld16(tb + 3 * NB + (uint32_t)n0, i1);
         tmem_wait_ld();
+        // the 16 columns' factors (whole warp, before the per-lane exit)
+        float spq[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) spq[q] = __shfl_sync(0xffffffffu, n0 < 32 ? sp0 : sp1, (n0 + q) & 31);
         if (xv >= a.S) continue;
 #pragma unroll
         for (int q = 0; q < 16; ++q) {
           const int wl = wl0 + n0 + q;
           if (wl >= a.c) break;
           float2* s2 = a.scratch + (size_t)wl * a.per + a.s1 + xo;
-          __stcg(s2, make_float2(r0[q] * sc, i0[q] * sc));
-          __stcg(s2 + fo, make_float2(r1[q] * sc, i1[q] * sc));
+          __stcg(s2, make_float2(r0[q] * spq[q], i0[q] * spq[q]));
+          __stcg(s2 + fo, make_float2(r1[q] * spq[q], i1[q] * spq[q]));
         }
       }
       // the accumulators t are free for item k + 2
@@ -364,15 +382,17 @@ srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, un
   return r == CUDA_SUCCESS ? SRK_OK : fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
 }
 
-// The row pass of one chunk of c work tiles: planes [2M][c][M] FP16 (k_p1h)
-// -> S2 of every work tile at scratch + wl*per + s1 (P3's layout).
-srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
-                          int P, cudaStream_t s) {
+// The row pass of one chunk of c work tiles: planes [2M][c][M] FP16 (k_p1h,
+// work tile wl scaled by 2^plane_exp(mx[wl])) -> S2 of every work tile at
+// scratch + wl*per + s1 (P3's layout).
+srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, const unsigned int* mx, int c, float2* scratch,
+                          size_t per, size_t s1, int S, int P, cudaStream_t s) {
   CUtensorMap map;
   SRK_TRY(tensor_rows_plane_map(planes, c, 64, hyb::NB, 1, &map, true));
   hyb::Args a;
   a.tabs = p->hyb_tabs;
   a.tab_exp = reinterpret_cast<const int*>(p->direct_err + 2);
+  a.mx = mx;
   a.scratch = scratch;
   a.per = per;
   a.s1 = s1;

@@ -98,6 +98,7 @@ struct srk_plan_s {
   size_t hyb_s1_bytes = 0;
   uint16_t* hyb_tabs = nullptr;
   double2* hyb_g = nullptr;
+  unsigned int* hyb_mx = nullptr;  // largest |Z| per work tile in flight (float bits): the planes' scales
   bool hyb_ready = false;
   float2* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -161,8 +162,8 @@ bool tensor_rows_supported(const srk_plan_s* p, std::string* why);
 size_t tensor_rows_tab_bytes(const srk_plan_s* p);
 size_t tensor_rows_g_bytes(const srk_plan_s* p);
 srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s);
-srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, int c, float2* scratch, size_t per, size_t s1, int S,
-                          int P, cudaStream_t s);
+srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, const unsigned int* mx, int c, float2* scratch,
+                          size_t per, size_t s1, int S, int P, cudaStream_t s);
 // Tensor map of a chunk's FP16 planes [2M][c][M] with the given box.
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
                                  CUtensorMap* out, bool swizzle128 = false);

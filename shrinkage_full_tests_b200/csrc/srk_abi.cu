@@ -480,7 +480,7 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->tw) cudaFree(p->tw);
   for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd,
                   (void*)p->kd[0], (void*)p->kd[1], (void*)p->direct_tabs, (void*)p->direct_err,
-                  (void*)p->hyb_s1, (void*)p->hyb_tabs, (void*)p->hyb_g})
+                  (void*)p->hyb_s1, (void*)p->hyb_tabs, (void*)p->hyb_g, (void*)p->hyb_mx})
     if (q) cudaFree(q);
   if (p->wbuf) cudaFree(p->wbuf);
   for (auto& kv : p->tables) {
@@ -530,6 +530,7 @@ srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
       SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_s1), bytes));
       p->hyb_s1_bytes = bytes;
     }
+    if (!p->hyb_mx) SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_mx), (size_t)p->chunk * sizeof(unsigned int)));
     p->schedule = sch;
     SRK_TRY(refresh_direct(p, nullptr));
     SRK_CUDA(cudaStreamSynchronize(nullptr));
@@ -572,7 +573,9 @@ srk_status srk_plan_sync(srk_plan p, srk_stream_t s) {
     SRK_CUDA(cudaMemcpy(&derr, p->direct_err, sizeof(derr), cudaMemcpyDeviceToHost));
     if (derr) {
       SRK_CUDA(cudaMemset(p->direct_err, 0, sizeof(derr)));
-      return fail(SRK_ERR_TIMEOUT, "a bounded wait of the direct schedule gave up (site %u); outputs incomplete",
+      return fail(SRK_ERR_TIMEOUT,
+                  "a tensor-core schedule stopped early (site %u: 1-13 a bounded wait gave up, 14-15 a shared "
+                  "memory block off its alignment); outputs incomplete",
                   derr);
     }
   }

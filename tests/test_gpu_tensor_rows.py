@@ -50,6 +50,77 @@ def test_tensor_rows_training_forward(torch_cuda, dt, N, KW, B, budget):
         assert rel_max_err(Rt[b], Rf[b]) < 1e-2, b
 
 
+@pytest.mark.parametrize("dt,amp", [("f16", 1e4), ("bf16", 1e8), ("bf16", 1e-20)])
+def test_tensor_rows_input_range(torch_cuda, dt, amp):
+    """Inputs far from [0, 1]: column spectra of an FP16 image scaled to 1e4
+    (or a BF16 one to 1e8) exceed FP16's range, those of a BF16 image scaled
+    to 1e-20 fall below it; the per-chunk plane scale keeps both within the
+    storage tolerance of the oracle (R is linear in E: the absolute floor
+    scales with amp)."""
+    torch = torch_cuda
+    sdt, tname = DT[dt]
+    tdt = getattr(torch, tname)
+    N, KW, B, dx = 512, 121, 2, 4.0
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    Kx, Ky = kernel(KW, "baseline", dx)
+    GX, GY = spectra(Kx, Ky, N, torch)
+    E = (dev(np.stack(fields(N, B, 70 + KW)), torch) * amp).to(tdt)
+    I = dev(np.stack(fields(N, B, 90 + KW)), torch).to(tdt)
+    out = {}
+    for sch in (srk.SRK_SCHEDULE_TENSOR_ROWS, srk.SRK_SCHEDULE_THREE_PASS):
+        plan = srk.SrkPlan(N, W, e, dx, B, dtype=sdt, tile_M=512)
+        plan.set_schedule(sch)
+        R = torch.full((B, W, W), float("nan"), device="cuda", dtype=tdt)
+        srk.srkTrainingForward(E, I, GX, GY, N, W, e, dx, B, None, R, plan)
+        plan.sync()
+        out[sch] = R.double().cpu().numpy()
+    Rt, Rf = out[srk.SRK_SCHEDULE_TENSOR_ROWS], out[srk.SRK_SCHEDULE_THREE_PASS]
+    assert np.isfinite(Rt).all()
+    Eh, Ih = E.double().cpu().numpy(), I.double().cpu().numpy()
+    for b in range(B):
+        ref = O.forward(Eh[b], Ih[b], Kx, Ky, e, dx)
+        assert rel_max_err(Rt[b], ref) < 1e-2, b
+        assert pixel_violations(Rt[b], ref, tol_abs=1e-3 * amp, tol_rel=1e-2) == 0, b
+        assert rel_max_err(Rt[b], Rf[b]) < 1e-2, b
+
+
+def test_tensor_rows_mixed_amplitudes_ring(torch_cuda):
+    """B = 600 (300 work tiles: three chunks through the two-slot pipeline,
+    the third reusing the first slot's planes and largest-|Z| words) with
+    the amplitude changing per image pair from 1e-3 to 1e4, so that work
+    tiles at scale 1 and refitted ones sit side by side in every chunk.
+    Every image against the FFT row pass; the extremes against the oracle."""
+    torch = torch_cuda
+    N, KW, B, dx = 512, 121, 600, 4.0
+    e = (KW - 1) // 2
+    W = N - 2 * e
+    Kx, Ky = kernel(KW, "baseline", dx)
+    GX, GY = spectra(Kx, Ky, N, torch)
+    amp = np.array([10.0 ** (((b // 2) * 3) % 8 - 3) for b in range(B)])
+    base = np.stack(fields(N, 16, 17))
+    E = (dev(base[np.arange(B) % 16], torch) * torch.from_numpy(amp).float().cuda()[:, None, None]).half()
+    I = dev(np.stack(fields(N, 16, 19))[np.arange(B)[::-1] % 16], torch).half()
+    out = {}
+    for sch in (srk.SRK_SCHEDULE_TENSOR_ROWS, srk.SRK_SCHEDULE_THREE_PASS):
+        plan = srk.SrkPlan(N, W, e, dx, B, dtype=srk.SRK_F16, tile_M=512)
+        plan.set_schedule(sch)
+        R = torch.full((B, W, W), float("nan"), device="cuda", dtype=torch.float16)
+        srk.srkTrainingForward(E, I, GX, GY, N, W, e, dx, B, None, R, plan)
+        plan.sync()
+        out[sch] = R.float().cpu().numpy()
+        if sch == srk.SRK_SCHEDULE_TENSOR_ROWS:
+            assert plan.info()["last_launches"] == 12  # three chunks of four launches
+    Rt, Rf = out[srk.SRK_SCHEDULE_TENSOR_ROWS], out[srk.SRK_SCHEDULE_THREE_PASS]
+    assert np.isfinite(Rt).all()
+    for b in range(B):
+        assert rel_max_err(Rt[b], Rf[b]) < 1e-2, (b, amp[b])
+    for b in (int(np.argmin(amp)), int(np.argmax(amp))):
+        ref = O.forward(E[b].double().cpu().numpy(), I[b].double().cpu().numpy(), Kx, Ky, e, dx)
+        assert rel_max_err(Rt[b], ref) < 1e-2, (b, amp[b])
+        assert pixel_violations(Rt[b], ref, tol_abs=1e-3 * amp[b], tol_rel=1e-2) == 0, (b, amp[b])
+
+
 @pytest.mark.parametrize("dt", ["f16", "bf16"])
 def test_tensor_rows_single_image_ops(torch_cuda, dt):
     """N = 4096, KW = 61 (81 forward tiles of 512): the OaS forward with
