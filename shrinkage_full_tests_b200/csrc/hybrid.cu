@@ -11,20 +11,24 @@
 // inverse column FFT and the epilogue (P3) are unchanged: U is written to S2
 // in P3's blocked FP32 layout.
 //
-// GEMM form per CTA (one ky, 128 outputs x' = e + 128 j .. , 64 work tiles):
+// GEMM form per item (one ky, 128 outputs x' = e + 128 j .., 128 work tiles):
 //   D[m][n] = sum_k T[m][k] Z_n[ky][128 j + k],  T[m][k] = g[m - k + e],
-// complex: Ur = Tr Zr - Ti Zi, Ui = Tr Zi + Ti Zr, four real MMAs per K step
-// and field (the minus sign by the instruction descriptor's negate-A bit).
+// complex: Ur = Tr Zr - Ti Zi, Ui = Tr Zi + Ti Zr, four real MMAs of
+// 128 x 128 x 16 per K step and field (the minus sign by the instruction
+// descriptor's negate-A bit).  N = 128 keeps the operand reads from shared
+// memory (A 4 KB + B 4 KB per MMA) within what the tensor cores can fetch
+// while they compute; N = 64 (A re-read for half the work) measured twice
+// as many shared-memory wavefronts per output.
 // * B (Z planes, FP16, written by k_p1h) by TMA with the 128-byte swizzle:
-//   box {64 columns x, 64 work tiles, 1 plane}, the K-major SWIZZLE_128B
-//   operand (4 boxes per part at e = 60).
+//   box {64 columns x, 128 work tiles, 1 plane}, the K-major SWIZZLE_128B
+//   operand, streamed through a ring of NS atoms of 64 columns.
 // * A (the band T) never materialised: rows reversed, one slot table of
 //   KT/8 + 16 slots x 128 bytes per (ky, field, part), read through a
 //   descriptor with leading = stride byte offset = 128 (direct.cu explains the
 //   identity).  Tables scaled by a power of two (max |g| in [8, 16)).
-// * Persistent, one CTA per SM: two shared-memory stages and two sets of
-//   4 x 64 TMEM accumulator columns (Gx re/im, Gy re/im), so the epilogue of
-//   one item (its S2 stores) overlaps the loads and MMAs of the next.
+// * Persistent, one CTA per SM; per item one pass per field over the same
+//   atoms, into that field's TMEM set (2 x 128 columns), so the S2 stores of
+//   one field overlap the MMAs of the other.
 // * Precision: FP16 operands (Z and g rounded once), FP32 accumulation — for
 //   the FP16/BF16 storage forms (rel 1e-2 / abs 1e-3).
 #include <cuda.h>
@@ -40,12 +44,13 @@ using namespace srk::tc;
 
 constexpr int M = 512;
 constexpr int MT = 128;        // outputs x' per tile = TMEM lanes
-constexpr int NB = 64;         // work tiles per MMA (N): 2 CTAs per SM (4 x 64 TMEM columns each)
+constexpr int NB = 128;        // work tiles per item = MMA N (128 x 128 x 16 MMAs)
+constexpr int NS = 5;          // ring slots of plane atoms
 #ifndef SRK_HYB_EPI_WARPS
 #define SRK_HYB_EPI_WARPS 4
 #endif
 constexpr int kEpiWarps = SRK_HYB_EPI_WARPS;      // a multiple of 4: each TMEM lane quarter split by columns
-static_assert(kEpiWarps >= 4 && kEpiWarps % 4 == 0 && kEpiWarps <= 16, "whole lane quarters, 16-column steps");
+static_assert(kEpiWarps >= 4 && kEpiWarps % 4 == 0 && NB / (kEpiWarps / 4) % 16 == 0, "whole lane quarters");
 constexpr int kThreadsH = 32 * (kEpiWarps + 2);    // + the load warp and the MMA warp
 constexpr int kLoadWarp = kEpiWarps, kMmaWarp = kEpiWarps + 1;
 constexpr int kMaxE = 64;
@@ -65,51 +70,57 @@ struct Args {
   int c, e, S, P;         // work tiles in the chunk, erosion, valid stride, S2 pitch
 };
 
-__host__ __device__ inline size_t stage_bytes(int e) {
-  const size_t bpart = (size_t)kt_of(e) * NB * 2;
-  return 2 * bpart + 4 * (size_t)qs_of(e) * 128;
-}
-__host__ __device__ inline size_t smem_bytes(int e) { return 1024 + 2 * stage_bytes(e); }
+// One plane atom: 64 columns x of NB work tiles, both parts (re, im), each
+// part a TMA box of NB rows x 128 bytes with the 128-byte swizzle.
+constexpr uint32_t kPartBytes = (uint32_t)NB * 128;
+constexpr uint32_t kAtomBytes = 2 * kPartBytes;
+// The band tables of one ky: 2 fields x 2 parts x QS slots of 128 bytes.
+__host__ __device__ inline size_t band_bytes(int e) { return 4 * (size_t)qs_of(e) * 128; }
+// barriers | NS atoms | 2 band buffers
+__host__ __device__ inline size_t smem_bytes(int e) { return 1024 + (size_t)NS * kAtomBytes + 2 * band_bytes(e); }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
 }
 
 // Persistent: one CTA per SM walks the items (x'-tile j, ky, batch of NB work
-// tiles) with a stride of the grid.  Two shared-memory stages (B planes + A
-// bands) and two TMEM accumulator sets let the loads of item k+1 and the
-// MMAs of item k+1 run while the epilogue of item k drains its accumulators.
-//   full[s]  : stage s loaded (TMA / bulk copy bytes)     empty[s] : stage s read by the MMAs (commit)
-//   tfull[t] : accumulators t complete (commit)           tempty[t]: accumulators t drained (every epilogue warp)
+// tiles) with a stride of the grid.  An item runs as two passes, one per
+// field, over the same resident planes, each into its own TMEM accumulator
+// set (2 x NB columns), so the epilogue of one field drains while the MMAs of
+// the other run.  The planes stream through a ring of NS atoms (a slot is
+// freed by the field-1 pass); the band tables of an item are double-buffered.
+//   zfull[s] : atom slot s loaded (TMA bytes)        zempty[s]: slot s read by both passes (commit)
+//   bfull[b] : band buffer b loaded (bulk copy)      bempty[b]: buffer b read (commit)
+//   tfull[f] : accumulators of field f complete      tempty[f]: drained (every epilogue warp)
 __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CUtensorMap zmap, Args a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int e = a.e, KT = kt_of(e), KB = KT / 64, QS = qs_of(e);
-  // B (one part): KB boxes of NB rows (work tiles) x 64 columns x (128 bytes,
-  // 128-byte swizzle) — the canonical K-major SWIZZLE_128B operand: 8-row
-  // groups 1024 bytes apart, K advanced by 32 bytes per MMA within an atom
-  const uint32_t boxB = (uint32_t)NB * 128;
-  const uint32_t bpart = (uint32_t)KB * boxB;
   const uint32_t tab = (uint32_t)QS * 128;      // one (field, part) band
-  const uint32_t stage = 2 * bpart + 4 * tab;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);  // [2]
-  uint64_t* empty = full + 2;                          // [2]
-  uint64_t* tfull = empty + 2;                         // [2]
-  uint64_t* tempty = tfull + 2;                        // [2]
+  uint64_t* zfull = reinterpret_cast<uint64_t*>(smem);  // [NS]
+  uint64_t* zempty = zfull + NS;                        // [NS]
+  uint64_t* bfull = zempty + NS;                        // [2]
+  uint64_t* bempty = bfull + 2;                         // [2]
+  uint64_t* tfull = bempty + 2;                         // [2]
+  uint64_t* tempty = tfull + 2;                         // [2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-  unsigned char* St = smem + 1024;
+  unsigned char* Zs = smem + 1024;                      // NS atoms (1024-byte aligned: swizzle atoms)
+  unsigned char* Ts = Zs + (size_t)NS * kAtomBytes;     // 2 band buffers
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntx = (a.S + MT - 1) / MT, nbatch = (a.c + NB - 1) / NB;
   const int items = ntx * M * nbatch;
   const unsigned long long lim = a.spin_limit;
 
   if (threadIdx.x == 0) {
-    // the swizzle atoms of the B boxes must sit on 1024-byte boundaries
-    *abort_flag = (smem_u32(St) & 1023u) != 0;
+    *abort_flag = (smem_u32(Zs) & 1023u) != 0;
     if (*abort_flag) atomicCAS(a.err, 0u, 14u);
+    for (int i = 0; i < NS; ++i) {
+      mbar_init(zfull + i, 1);
+      mbar_init(zempty + i, 1);
+    }
     for (int i = 0; i < 2; ++i) {
-      mbar_init(full + i, 1);
-      mbar_init(empty + i, 1);
+      mbar_init(bfull + i, 1);
+      mbar_init(bempty + i, 1);
       mbar_init(tfull + i, 1);
       mbar_init(tempty + i, kEpiWarps);
     }
@@ -117,7 +128,7 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
   }
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(8 * NB));
+                 "r"(4 * NB));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -133,130 +144,153 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
 
   if (warp == kLoadWarp) {
     if (lane == 0) {
-      int issued = 0;
-      for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
-        const int s = k & 1;
-        if (k >= 2 && !mbar_wait(empty + s, (unsigned)((k / 2 - 1) & 1), lim)) {
-          atomicCAS(a.err, 0u, 13u);
-          *abort_flag = 1;
-        }
-        if (*abort_flag) break;
+      long long r = 0;  // atoms issued
+      int nb = 0;       // band buffers issued
+      for (int k = 0, item = blockIdx.x; item < items && !*abort_flag; ++k, item += gridDim.x) {
         int j, ky, batch;
         decode(item, j, ky, batch);
-        unsigned char* Bs = St + (size_t)s * stage;
-        mbar_expect_tx(full + s, stage);
-        for (int part = 0; part < 2; ++part)
-          for (int kb = 0; kb < KB; ++kb)
-            tma_load_3d(Bs + part * bpart + kb * boxB, &zmap, MT * j + 64 * kb, NB * batch, ky * 2 + part, full + s);
-        bulk_g2s(Bs + 2 * bpart, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, full + s);
-        ++issued;
+        const int b = k & 1;
+        if (k >= 2 && !mbar_wait(bempty + b, (unsigned)((k / 2 - 1) & 1), lim)) {
+          atomicCAS(a.err, 0u, 13u);
+          *abort_flag = 1;
+          break;
+        }
+        mbar_expect_tx(bfull + b, 4 * tab);
+        bulk_g2s(Ts + (size_t)b * 4 * tab, a.tabs + (size_t)ky * 4 * QS * 64, 4 * tab, bfull + b);
+        ++nb;
+        for (int at = 0; at < KB; ++at) {
+          const int slot = (int)(r % NS);
+          if (r >= NS && !mbar_wait(zempty + slot, (unsigned)((r / NS - 1) & 1), lim)) {
+            atomicCAS(a.err, 0u, 13u);
+            *abort_flag = 1;
+            break;
+          }
+          unsigned char* Zd = Zs + (size_t)slot * kAtomBytes;
+          mbar_expect_tx(zfull + slot, kAtomBytes);
+          for (int part = 0; part < 2; ++part)
+            tma_load_3d(Zd + part * kPartBytes, &zmap, MT * j + 64 * at, NB * batch, ky * 2 + part, zfull + slot);
+          ++r;
+        }
       }
-      // every copy has landed before the CTA can leave (also on the error path)
-      for (int k = issued > 2 ? issued - 2 : 0; k < issued; ++k) mbar_wait(full + (k & 1), (unsigned)((k / 2) & 1), lim);
+      // every copy issued has landed before the CTA can leave (also on the error path)
+      for (long long q = r > NS ? r - NS : 0; q < r; ++q) mbar_wait(zfull + (int)(q % NS), (unsigned)((q / NS) & 1), lim);
+      for (int q = nb > 2 ? nb - 2 : 0; q < nb; ++q) mbar_wait(bfull + (q & 1), (unsigned)((q / 2) & 1), lim);
     }
     __syncwarp();
   } else if (warp == kMmaWarp) {
     if (lane == 0) {
       const uint32_t id = idesc_f16(0, MT, NB);
       const uint32_t idn = id | (1u << 13);  // negate A
-      for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
-        const int s = k & 1, t = k & 1;
-        if (!mbar_wait(full + s, (unsigned)((k / 2) & 1), lim) ||
-            (k >= 2 && !mbar_wait(tempty + t, (unsigned)((k / 2 - 1) & 1), lim))) {
-          atomicCAS(a.err, 0u, 11u);
-          *abort_flag = 1;
-        }
-        if (*abort_flag) break;
-        tc_fence_after();
-        const uint32_t b0 = smem_u32(St + (size_t)s * stage), a0 = b0 + 2 * bpart;
-        const uint32_t d0 = tmem + (uint32_t)t * 4 * NB;
-        for (int ks = 0; ks < KT / 16; ++ks) {
-          const uint32_t boff = (uint32_t)(ks >> 2) * boxB + (uint32_t)(ks & 3) * 32;
-          const uint64_t dbr = sdesc_sw128(b0 + boff);
-          const uint64_t dbi = sdesc_sw128(b0 + bpart + boff);
+      long long r = 0;                       // first atom of the item
+      bool ok = true;
+      for (int k = 0, item = blockIdx.x; item < items && ok; ++k, item += gridDim.x, r += KB) {
+        const int b = k & 1;
+        ok = mbar_wait(bfull + b, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
+        const uint32_t a0 = smem_u32(Ts + (size_t)b * 4 * tab);
+        for (int f = 0; f < 2 && ok; ++f) {
+          // accumulator set f, drained by the epilogue of the previous item's field f
+          if (k >= 1 && !mbar_wait(tempty + f, (unsigned)((k - 1) & 1), lim)) ok = false;
+          const uint32_t dr = tmem + (uint32_t)f * 2 * NB, di = dr + NB;
+          for (int at = 0; at < KB && ok; ++at) {
+            const long long q = r + at;
+            const int slot = (int)(q % NS);
+            if (f == 0 && !mbar_wait(zfull + slot, (unsigned)((q / NS) & 1), lim)) ok = false;
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t b0 = smem_u32(Zs + (size_t)slot * kAtomBytes);
 #pragma unroll
-          for (int f = 0; f < 2; ++f) {
-            const uint64_t dar = sdesc(a0 + (uint32_t)(f * 2 + 0) * tab + (uint32_t)ks * 256, 128, 128);
-            const uint64_t dai = sdesc(a0 + (uint32_t)(f * 2 + 1) * tab + (uint32_t)ks * 256, 128, 128);
-            const uint32_t dr = d0 + (uint32_t)(f * 2 + 0) * NB, di = d0 + (uint32_t)(f * 2 + 1) * NB;
-            mma_f16(dr, dar, dbr, id, ks > 0);   // + Tr Zr
-            mma_f16(dr, dai, dbi, idn, true);    // - Ti Zi
-            mma_f16(di, dar, dbi, id, ks > 0);   // + Tr Zi
-            mma_f16(di, dai, dbr, id, true);     // + Ti Zr
+            for (int kk = 0; kk < 4; ++kk) {
+              const int ks = 4 * at + kk;
+              const uint64_t dbr = sdesc_sw128(b0 + (uint32_t)kk * 32);
+              const uint64_t dbi = sdesc_sw128(b0 + kPartBytes + (uint32_t)kk * 32);
+              const uint64_t dar = sdesc(a0 + (uint32_t)(f * 2 + 0) * tab + (uint32_t)ks * 256, 128, 128);
+              const uint64_t dai = sdesc(a0 + (uint32_t)(f * 2 + 1) * tab + (uint32_t)ks * 256, 128, 128);
+              mma_f16(dr, dar, dbr, id, ks > 0);   // + Tr Zr
+              mma_f16(dr, dai, dbi, idn, true);    // - Ti Zi
+              mma_f16(di, dar, dbi, id, ks > 0);   // + Tr Zi
+              mma_f16(di, dai, dbr, id, true);     // + Ti Zr
+            }
+            if (f == 1) mma_commit(zempty + slot);  // both passes have read the atom
           }
+          if (ok) mma_commit(tfull + f);
         }
-        mma_commit(empty + s);  // stage s free once these MMAs have read it
-        mma_commit(tfull + t);  // accumulators t complete
+        if (ok) mma_commit(bempty + b);
+      }
+      if (!ok) {
+        atomicCAS(a.err, 0u, 11u);
+        *abort_flag = 1;
       }
     }
     __syncwarp();
   } else {
     // epilogue warp: TMEM lane quarter (warp % 4) and its share of the NB columns
     constexpr int kCols = NB / (kEpiWarps / 4);
+    static_assert(NB == 128, "four column factors per lane");
     const int quarter = warp & 3, colh = warp >> 2;
     const int mrow = quarter * 32 + lane;         // TMEM lane (rows reversed)
     const int tab_exp = __ldg(a.tab_exp);
     const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
     const size_t fo = (size_t)a.P * M;            // S2 field stride
-    for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
-      const int t = k & 1;
+    bool ok = true;
+    for (int k = 0, item = blockIdx.x; item < items && ok; ++k, item += gridDim.x) {
       int j, ky, batch;
       decode(item, j, ky, batch);
       const int wl0 = NB * batch;
-      // the largest |Z| words of the NB work tiles (columns lane, lane + 32),
-      // loaded before the wait for the accumulators so that their latency hides behind it
-      static_assert(NB == 64, "two column factors per lane");
-      const unsigned int z0 = __ldg(a.mx + min(wl0 + lane, a.c - 1));
-      const unsigned int z1 = __ldg(a.mx + min(wl0 + 32 + lane, a.c - 1));
-      bool ok = true;
-      if (lane == 0) ok = mbar_wait(tfull + t, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
-      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-      if (!ok) {
-        if (lane == 0) {
-          atomicCAS(a.err, 0u, 12u);
-          *abort_flag = 1;
-        }
-        break;
-      }
-      tc_fence_after();
+      // largest |Z| words of the columns lane + 32 h, loaded before the wait so their latency hides behind it
+      unsigned int zw[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) zw[h] = __ldg(a.mx + min(wl0 + 32 * h + lane, a.c - 1));
       const int xv = MT * j + MT - 1 - mrow;      // valid-column index x' - e
       const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)ky * 4 + (xv & 3);
-      const uint32_t tb = trow + (uint32_t)t * 4 * NB;
-      // the column factors 2^-(p + tab_exp)
-      const float sp0 = ldexpf(1.f, -plane_exp(z0) - tab_exp);
-      const float sp1 = ldexpf(1.f, -plane_exp(z1) - tab_exp);
-      for (int n0 = colh * kCols; n0 < (colh + 1) * kCols; n0 += 16) {
-        float r0[16], i0[16], r1[16], i1[16];
-        tmem_ld16(tb + 0 * NB + (uint32_t)n0, r0);
-        tmem_ld16(tb + 1 * NB + (uint32_t)n0, i0);
-        tmem_ld16(tb + 2 * NB + (uint32_t)n0, r1);
-        tmem_ld16(tb + 3 * NB + (uint32_t)n0, i1);
-        tmem_wait_ld();
-        // the 16 columns' factors (whole warp, before the per-lane exit)
-        float spq[16];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) spq[q] = __shfl_sync(0xffffffffu, n0 < 32 ? sp0 : sp1, (n0 + q) & 31);
-        if (xv >= a.S) continue;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int wl = wl0 + n0 + q;
-          if (wl >= a.c) break;
-          float2* s2 = a.scratch + (size_t)wl * a.per + a.s1 + xo;
-          __stcg(s2, make_float2(r0[q] * spq[q], i0[q] * spq[q]));
-          __stcg(s2 + fo, make_float2(r1[q] * spq[q], i1[q] * spq[q]));
+      float sp[4];
+      for (int f = 0; f < 2; ++f) {
+        bool w = true;
+        if (lane == 0) w = mbar_wait(tfull + f, (unsigned)(k & 1), lim) && !*abort_flag;
+        if (__shfl_sync(0xffffffffu, w ? 1 : 0, 0) == 0) {
+          if (lane == 0) {
+            atomicCAS(a.err, 0u, 12u);
+            *abort_flag = 1;
+          }
+          ok = false;
+          break;
         }
+        tc_fence_after();
+        if (f == 0) {
+#pragma unroll
+          for (int h = 0; h < 4; ++h) sp[h] = ldexpf(1.f, -plane_exp(zw[h]) - tab_exp);  // 2^-(p + tab_exp)
+        }
+        const uint32_t tb = trow + (uint32_t)f * 2 * NB;
+        float2* out = a.scratch + a.s1 + xo + (size_t)f * fo;
+        for (int n0 = colh * kCols; n0 < (colh + 1) * kCols; n0 += 16) {
+          float re[16], im[16];
+          tmem_ld16(tb + (uint32_t)n0, re);
+          tmem_ld16(tb + NB + (uint32_t)n0, im);
+          tmem_wait_ld();
+          // the 16 columns' factors (whole warp, before the per-lane exit)
+          const float spn = n0 < 64 ? (n0 < 32 ? sp[0] : sp[1]) : (n0 < 96 ? sp[2] : sp[3]);
+          float spq[16];
+#pragma unroll
+          for (int q = 0; q < 16; ++q) spq[q] = __shfl_sync(0xffffffffu, spn, (n0 + q) & 31);
+          if (xv >= a.S) continue;
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int wl = wl0 + n0 + q;
+            if (wl >= a.c) break;
+            __stcg(out + (size_t)wl * a.per, make_float2(re[q] * spq[q], im[q] * spq[q]));
+          }
+        }
+        // accumulators f are free for the next item
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(tempty + f);
       }
-      // the accumulators t are free for item k + 2
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(tempty + t);
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == kMmaWarp) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(8 * NB));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * NB));
   }
 }
 
