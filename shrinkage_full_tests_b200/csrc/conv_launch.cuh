@@ -29,7 +29,7 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   const size_t smp1 = p1h_smem_bytes();
   const size_t sm3 = phase_smem_bytes<M>() + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
   SRK_TRY(set_smem(k_p1h<OP, T>, smp1));
-  SRK_TRY(set_smem(k_p3<M, OP, T>, sm3));
+  SRK_TRY(set_smem(k_p3<M, OP, T, true>, sm3));
   SRK_TRY(set_smem(k_p1h_refit<OP, T>, smp1));
   int chunk = 0;  // work tiles per slot (two slots in the pipelined form)
   // largest |Z| of the work tiles of the chunk in slot k & 1 (their planes' scales)
@@ -45,7 +45,7 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
     return SRK_OK;
   };
   auto p3 = [&](int w0, int c, float2* base, cudaStream_t st) {
-    k_p3<M, OP, T><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, st>>>(base, a, g, p->tw, w0, p->nsm);
+    k_p3<M, OP, T, true><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, st>>>(base, a, g, p->tw, w0, p->nsm);
   };
   const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
   int launches = 0;

@@ -947,6 +947,34 @@ __device__ __forceinline__ void stage_rows(const float2* __restrict__ src, int p
   }
 }
 
+// stage_rows for a rotated S2 block (the tensor-core row pass's layout):
+// block line y holds frequency row (y - rot) mod M, which lands in the rows
+// at that index.  Rotating the lines by the column block spreads the row
+// pass's 32-byte pieces of one ky over the L2 instead of stacking them at one
+// offset of blocks 16 KB apart.
+template <int M>
+__device__ __forceinline__ void stage_rows_rot(const float2* __restrict__ src, int rot, float2* __restrict__ rows) {
+  constexpr int RS = row_stride<M>();
+  constexpr int LPU = lpu_of<M>();
+  constexpr int Q = LPU / 2;
+  constexpr int NIT = M * Q / kThreads;
+  constexpr int YS = kThreads / Q;
+  const int y0 = threadIdx.x / Q, cp = threadIdx.x % Q;
+  const float4* sp = reinterpret_cast<const float4*>(src + (size_t)y0 * LPU + 2 * cp);
+  constexpr size_t sstep = (size_t)YS * LPU / 2;
+  float4 q[NIT];
+#pragma unroll
+  for (int j = 0; j < NIT; ++j) q[j] = __ldcg(sp + j * sstep);
+  float2* r0 = rows + (2 * cp) * RS;
+  float2* r1 = r0 + RS;
+#pragma unroll
+  for (int j = 0; j < NIT; ++j) {
+    const int ky = (y0 + j * YS - rot) & (M - 1);
+    r0[fft_pad(ky)] = make_float2(q[j].x, q[j].y);
+    r1[fft_pad(ky)] = make_float2(q[j].z, q[j].w);
+  }
+}
+
 // P2: rows ky0 .. ky0+LPU-1: FFT along x, spectral map, inverse, keep the
 // valid columns, write S2 rows.  All threads of the CTA take part.
 template <int M, int OP>
@@ -1050,7 +1078,7 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
 // still join the barriers).  For the forward and tangent epilogues with
 // erosion >= 1 the image columns the central differences need are staged in
 // shared memory after the transforms, in the rows they no longer use.
-template <int M, int OP, typename T, bool ASYNC = false>
+template <int M, int OP, typename T, bool ASYNC = false, bool ROT = false>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
                                        T* __restrict__ win0 = nullptr) {
@@ -1104,7 +1132,10 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   }
 #pragma unroll
   for (int l = 0; l < L; ++l) {
-    if constexpr (s2_blocked<M>())
+    if constexpr (ROT) {
+      static_assert(s2_blocked<M>(), "rotated blocks of the blocked layout");
+      stage_rows_rot<M>(S2 + ((size_t)l * (P / LPU) + xb) * M * LPU, xb & (M - 1), rows + l * LPU * RS);
+    } else if constexpr (s2_blocked<M>())
       stage_rows<M>(S2 + ((size_t)l * (P / LPU) + xb) * M * LPU, LPU, rows + l * LPU * RS);
     else
       stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
@@ -1216,7 +1247,8 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
                 rows + 2 * lpu_of<M>() * row_stride<M>());
 }
 
-template <int M, int OP, typename T>
+// ROT: S2 blocks rotated by the column block (written by the tensor-core row pass).
+template <int M, int OP, typename T, bool ROT = false>
 __global__ void __launch_bounds__(kThreads, SRK_P3_MIN_BLOCKS)
 k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0, int ahead) {
   extern __shared__ float2 sm[];
@@ -1250,7 +1282,7 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
       }
     }
   }
-  phase3<M, OP, T, ASYNC>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
+  phase3<M, OP, T, ASYNC, ROT>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
                           sm + tw_slots<M>(), sm, line, t, win0);
 }
 
