@@ -3,6 +3,7 @@
 #pragma once
 #include "internal.h"
 #include "hybrid_p1.cuh"
+#include "hybrid_p1g.cuh"
 
 namespace srk {
 
@@ -14,10 +15,11 @@ srk_status set_smem(K kernel, size_t bytes) {
 }
 
 // Three-pass schedule with the tensor-core row pass (SRK_SCHEDULE_TENSOR_ROWS):
-// per chunk P1h (column FFT -> FP16 planes, with each work tile's largest
-// |Z|) and its refit pass (the work tiles outside FP16's comfortable range
-// again, scaled by a power of two), the row pass of hybrid.cu (-> S2), P3
-// unchanged; two slots of chunks on two streams.
+// per chunk the column pass (-> FP16 planes, with each work tile's largest
+// |Z|: the column DFT on the tensor cores, k_p1g, where its TMA boxes apply,
+// else the column FFT, k_p1h) and its refit pass (the work tiles outside
+// FP16's comfortable range again, scaled by a power of two), the row pass of
+// hybrid.cu (-> S2), P3; two slots of chunks on two streams.
 template <int OP, typename T>
 srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, cudaStream_t s) {
   constexpr int M = kHybM;
@@ -29,8 +31,20 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
   const size_t smp1 = p1h_smem_bytes();
   const size_t sm3 = phase_smem_bytes<M>() + (p3_async_window<OP, T>() ? sizeof(float) * p3_window_floats<M>() : 0);
   SRK_TRY(set_smem(k_p1h<OP, T>, smp1));
-  SRK_TRY(set_smem(k_p3<M, OP, T, true>, sm3));
+  SRK_TRY(set_smem(k_p3<M, OP, T, kHybS2Layout>, sm3));
   SRK_TRY(set_smem(k_p1h_refit<OP, T>, smp1));
+  static_assert(OpTraits<OP>::PAIRS, "the tensor-row schedule serves the pair ops");
+  // k_p1g (column DFT on the tensor cores): a uniform batch, N % 8 == 0
+  // (16-byte image rows), tile origins on 8-row boundaries (TMA's innermost
+  // coordinate), a 16-byte aligned image array; else the column FFT, k_p1h
+  const int nimg = g.TT > 0 ? g.U / g.TT : 0;
+  const bool dft = p->p1g_tab && !g.rtile && g.N % 8 == 0 && (g.TT == 1 || g.S % 8 == 0) &&
+                   (reinterpret_cast<uintptr_t>(a.E) & 15) == 0;
+  CUtensorMap tmapg, smapg;
+  if (dft) {
+    SRK_TRY(set_smem(p1g::k_p1g<T>, p1g::smem_bytes()));
+    SRK_TRY(tensor_rows_p1g_maps(p, a.E, g.N, nimg, &tmapg, &smapg));
+  }
   int chunk = 0;  // work tiles per slot (two slots in the pipelined form)
   // largest |Z| of the work tiles of the chunk in slot k & 1 (their planes' scales)
   auto max_of = [&](int k) { return p->hyb_mx + (size_t)(k & 1) * chunk; };
@@ -38,14 +52,31 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
     CUtensorMap pmap;
     SRK_TRY(tensor_rows_plane_map(planes, c, kP1hCols, 1, kP1hBox, &pmap));
     SRK_CUDA(cudaMemsetAsync(max_of(k), 0, (size_t)c * sizeof(unsigned int), st));
-    k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, p->nsm, max_of(k),
-                                                                 p->direct_err);
+    if (dft) {
+      CUtensorMap pmapg;  // 256 plane rows x 64 columns, 128-byte swizzle
+      SRK_TRY(tensor_rows_plane_map(planes, c, p1g::XB, 1, 256, &pmapg, true));
+      p1g::Args ga;
+      ga.planes = planes;
+      ga.zmax = max_of(k);
+      ga.err = p->direct_err;
+      ga.spin_limit = 1ull << 22;
+      ga.g = g;
+      ga.w0 = w0;
+      ga.c = c;
+      ga.nimg = nimg;
+      const int items = c * (p1g::M / p1g::XB) * 2;
+      p1g::k_p1g<T><<<std::min(items, std::max(p->nsm, 1)), p1g::kThreadsG, p1g::smem_bytes(), st>>>(
+          tmapg, smapg, pmapg, ga);
+    } else {
+      k_p1h<OP, T><<<dim3(M / kP1hCols, c), kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, p->nsm, max_of(k),
+                                                                   p->direct_err);
+    }
     k_p1h_refit<OP, T><<<std::max(p->nsm, 1) * 2, kThreads, smp1, st>>>(pmap, a, g, p->tw, w0, c, max_of(k),
                                                                         p->direct_err);
     return SRK_OK;
   };
   auto p3 = [&](int w0, int c, float2* base, cudaStream_t st) {
-    k_p3<M, OP, T, true><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, st>>>(base, a, g, p->tw, w0, p->nsm);
+    k_p3<M, OP, T, kHybS2Layout><<<dim3((g.S + LPU - 1) / LPU, c), kThreads, sm3, st>>>(base, a, g, p->tw, w0, p->nsm);
   };
   const int whole = (int)std::min<size_t>(std::max<size_t>(cap, 1), 65535);
   int launches = 0;
@@ -93,7 +124,12 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
 
 template <int M, int OP, typename T>
 srk_status launch_conv_m(srk_plan_s* p, const OpArgs& a, const Geom& g, int nwt, bool conjG, cudaStream_t s) {
-  if constexpr (M == kHybM && OpTraits<OP>::K == 1 && !std::is_same<T, float>::value) {
+  // the tensor-core row pass serves the pair ops (forward, VJP); a tangent
+  // field packed beside its primal in one complex column loses too much to
+  // the FP16 planes (measured past the per-pixel tolerance on the
+  // tangent-adjoint at N = 1024, KW = 121), so JVP and tangent-adjoint run
+  // the FFT schedule on such a plan
+  if constexpr (M == kHybM && OpTraits<OP>::K == 1 && OpTraits<OP>::PAIRS && !std::is_same<T, float>::value) {
     if (p->schedule == SRK_SCHEDULE_TENSOR_ROWS && p->hyb_ready) return launch_tensor_rows<OP, T>(p, a, g, nwt, s);
   }
   const size_t sm1 = phase_smem_bytes<M>();

@@ -1078,7 +1078,11 @@ __device__ __forceinline__ void phase2(const float2* __restrict__ S1, float2* __
 // still join the barriers).  For the forward and tangent epilogues with
 // erosion >= 1 the image columns the central differences need are staged in
 // shared memory after the transforms, in the rows they no longer use.
-template <int M, int OP, typename T, bool ASYNC = false, bool ROT = false>
+// S2 layouts P3 reads: the engine's (blocked for M = 512), the blocked one
+// with rotated lines, or the plain one [field][ky][P] (the latter two written
+// by the tensor-core row pass).
+enum S2Layout : int { kS2Engine = 0, kS2Rotated = 1, kS2Plain = 2 };
+template <int M, int OP, typename T, bool ASYNC = false, int S2L = kS2Engine>
 __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpArgs& a, const Geom& g, int w, int xb,
                                        float2* __restrict__ rows, const float2* __restrict__ tw, int line, int t,
                                        T* __restrict__ win0 = nullptr) {
@@ -1132,10 +1136,10 @@ __device__ __forceinline__ void phase3(const float2* __restrict__ S2, const OpAr
   }
 #pragma unroll
   for (int l = 0; l < L; ++l) {
-    if constexpr (ROT) {
+    if constexpr (S2L == kS2Rotated) {
       static_assert(s2_blocked<M>(), "rotated blocks of the blocked layout");
       stage_rows_rot<M>(S2 + ((size_t)l * (P / LPU) + xb) * M * LPU, xb & (M - 1), rows + l * LPU * RS);
-    } else if constexpr (s2_blocked<M>())
+    } else if constexpr (s2_blocked<M>() && S2L == kS2Engine)
       stage_rows<M>(S2 + ((size_t)l * (P / LPU) + xb) * M * LPU, LPU, rows + l * LPU * RS);
     else
       stage_rows<M>(S2 + (size_t)l * M * P + x0, P, rows + l * LPU * RS);
@@ -1247,8 +1251,8 @@ k_p2(float2* __restrict__ scratch, const float2* __restrict__ Gx, const float2* 
                 rows + 2 * lpu_of<M>() * row_stride<M>());
 }
 
-// ROT: S2 blocks rotated by the column block (written by the tensor-core row pass).
-template <int M, int OP, typename T, bool ROT = false>
+// S2L: the S2 layout (S2Layout).
+template <int M, int OP, typename T, int S2L = kS2Engine>
 __global__ void __launch_bounds__(kThreads, SRK_P3_MIN_BLOCKS)
 k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ twg, int w0, int ahead) {
   extern __shared__ float2 sm[];
@@ -1267,7 +1271,7 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
     const int by2 = lin / (int)gridDim.x, bx2 = lin % (int)gridDim.x;
     if (ahead > 0 && by2 < (int)gridDim.y) {
       const float2* s2 = scratch + by2 * wt_elems<M, OP>(g.S) + s1_elems<M, OP>();
-      if constexpr (s2_blocked<M>()) {
+      if constexpr (s2_blocked<M>() && S2L != kS2Plain) {
         constexpr int LINES = M * lpu_of<M>() * (int)sizeof(float2) / 128;  // per field
         static_assert(L * LINES <= kThreads, "one line per thread");
         if (threadIdx.x < L * LINES) {
@@ -1282,7 +1286,7 @@ k_p3(float2* __restrict__ scratch, OpArgs a, Geom g, const float2* __restrict__ 
       }
     }
   }
-  phase3<M, OP, T, ASYNC, ROT>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
+  phase3<M, OP, T, ASYNC, S2L>(scratch + wl * wt_elems<M, OP>(g.S) + s1_elems<M, OP>(), a, g, w0 + wl, blockIdx.x,
                           sm + tw_slots<M>(), sm, line, t, win0);
 }
 

@@ -37,6 +37,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include "hybrid_p1g.cuh"
 #include "hybrid_scale.cuh"
 #include "internal.h"
 #include "tc.cuh"
@@ -246,8 +247,11 @@ __global__ void __launch_bounds__(kThreadsH, 1) k_p2h(const __grid_constant__ CU
 #pragma unroll
       for (int h = 0; h < 4; ++h) zw[h] = __ldg(a.mx + min(wl0 + 32 * h + lane, a.c - 1));
       const int xv = MT * j + MT - 1 - mrow;      // valid-column index x' - e
-      // S2 block xv >> 2 holds ky at line (ky + xv >> 2) mod M (k_p3<.., ROT = true>)
-      const size_t xo = (size_t)(xv >> 2) * M * 4 + (size_t)((ky + (xv >> 2)) & (M - 1)) * 4 + (xv & 3);
+      // rotated blocked layout: S2 block xv >> 2 holds ky at line (ky + xv >> 2) mod M;
+      // plain layout: row ky, column xv
+      const size_t xo = kHybS2Layout == 2
+                            ? (size_t)ky * a.P + xv
+                            : (size_t)(xv >> 2) * M * 4 + (size_t)((ky + (xv >> 2)) & (M - 1)) * 4 + (xv & 3);
       float sp[4];
       for (int f = 0; f < 2; ++f) {
         bool w = true;
@@ -405,6 +409,50 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn_h() {
   return fn;
 }
 }  // namespace
+
+// The column-DFT tables of k_p1g (C and S rows, 512 KB), in the plan's storage type.
+size_t tensor_rows_p1g_tab_bytes() { return (size_t)2 * (p1g::M / 2) * p1g::M * 2; }
+srk_status tensor_rows_p1g_tables(srk_plan_s* p, cudaStream_t s) {
+  const int n = 2 * (p1g::M / 2) * p1g::M;
+  if (p->dtype == SRK_BF16)
+    p1g::k_p1g_tables<__nv_bfloat16><<<(n + 255) / 256, 256, 0, s>>>(static_cast<__nv_bfloat16*>(p->p1g_tab));
+  else
+    p1g::k_p1g_tables<__half><<<(n + 255) / 256, 256, 0, s>>>(static_cast<__half*>(p->p1g_tab));
+  return cuda_status(cudaGetLastError(), "column-DFT tables");
+}
+
+// Tensor maps of k_p1g: the tables (box 64 y x 128 rows) and the images
+// ([nimg][N][N] column-major, box 64 y x 64 x x 1), both with the 128-byte
+// swizzle.  The caller checks N % 8 == 0 and a 16-byte aligned image array.
+srk_status tensor_rows_p1g_maps(const srk_plan_s* p, const void* img, int N, int nimg, CUtensorMap* tmap,
+                                CUtensorMap* smap) {
+  auto enc = encode_fn_h();
+  if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+  const CUtensorMapDataType dt = p->dtype == SRK_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  {
+    std::memset(tmap, 0, sizeof(*tmap));
+    const cuuint64_t dims[2] = {(cuuint64_t)p1g::M, (cuuint64_t)p1g::M};
+    const cuuint64_t strides[1] = {(cuuint64_t)p1g::M * 2};
+    const cuuint32_t box[2] = {64, (cuuint32_t)p1g::KR};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(tmap, dt, 2, p->p1g_tab, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled (DFT tables) failed (%d)", (int)r);
+  }
+  {
+    std::memset(smap, 0, sizeof(CUtensorMap));
+    const cuuint64_t dims[3] = {(cuuint64_t)N, (cuuint64_t)N, (cuuint64_t)nimg};
+    const cuuint64_t strides[2] = {(cuuint64_t)N * 2, (cuuint64_t)N * N * 2};
+    const cuuint32_t box[3] = {64, (cuuint32_t)p1g::XB, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = enc(smap, dt, 3, const_cast<void*>(img), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled (images) failed (%d)", (int)r);
+  }
+  return SRK_OK;
+}
 
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
                                  CUtensorMap* out, bool swizzle128) {

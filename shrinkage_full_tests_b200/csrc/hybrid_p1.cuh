@@ -6,9 +6,9 @@
 // c = work tiles in the chunk, wl = work tile within the chunk.  Each CTA
 // transforms 8 consecutive columns (two units of four), stages their values
 // [ky][part][8] in shared memory and writes them with TMA stores (one
-// 16-byte piece per (ky, part) plane row).  Only for single-field
-// ops (one complex field per work tile: OP_FWD, OP_VJP_F, OP_JVP,
-// OP_TANADJ_F).
+// 16-byte piece per (ky, part) plane row).  Used for the pair ops (OP_FWD,
+// OP_VJP_F: two images per work tile) where the column DFT of
+// hybrid_p1g.cuh does not apply, and by the refit pass.
 #pragma once
 #include <cuda.h>
 

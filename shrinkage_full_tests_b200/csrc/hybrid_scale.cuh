@@ -6,6 +6,13 @@
 
 namespace srk {
 
+// S2 layout the row pass writes and P3 reads (S2Layout in engine.cuh):
+// 1 = blocked with rotated lines, 2 = plain [field][ky][pitch].
+#ifndef SRK_HYB_S2_LAYOUT
+#define SRK_HYB_S2_LAYOUT 1
+#endif
+constexpr int kHybS2Layout = SRK_HYB_S2_LAYOUT;
+
 // FP16 range of the planes.  A column spectrum value is a sum of M = 512
 // complex inputs (|Z.x|, |Z.y| <= 2^10 max|input|) and FP16 holds at most
 // 65504 with full precision only above 2^-14: unscaled, an FP16 or BF16

@@ -99,6 +99,7 @@ struct srk_plan_s {
   uint16_t* hyb_tabs = nullptr;
   double2* hyb_g = nullptr;
   unsigned int* hyb_mx = nullptr;  // largest |Z| per work tile in flight (float bits): the planes' scales
+  void* p1g_tab = nullptr;         // column-DFT tables of the tensor-core column pass (storage type)
   bool hyb_ready = false;
   float2* scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -164,6 +165,10 @@ size_t tensor_rows_g_bytes(const srk_plan_s* p);
 srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s);
 srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, const unsigned int* mx, int c, float2* scratch,
                           size_t per, size_t s1, int S, int P, cudaStream_t s);
+size_t tensor_rows_p1g_tab_bytes();
+srk_status tensor_rows_p1g_tables(srk_plan_s* p, cudaStream_t s);
+srk_status tensor_rows_p1g_maps(const srk_plan_s* p, const void* img, int N, int nimg, CUtensorMap* tmap,
+                                CUtensorMap* smap);
 // Tensor map of a chunk's FP16 planes [2M][c][M] with the given box.
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,
                                  CUtensorMap* out, bool swizzle128 = false);

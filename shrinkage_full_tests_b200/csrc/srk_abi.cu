@@ -480,7 +480,7 @@ srk_status srk_plan_destroy(srk_plan p) {
   if (p->tw) cudaFree(p->tw);
   for (void* q : {(void*)p->imp_tab, (void*)p->imp_tabr, (void*)p->imp_P, (void*)p->imp_Tm, (void*)p->imp_Kd,
                   (void*)p->kd[0], (void*)p->kd[1], (void*)p->direct_tabs, (void*)p->direct_err,
-                  (void*)p->hyb_s1, (void*)p->hyb_tabs, (void*)p->hyb_g, (void*)p->hyb_mx})
+                  (void*)p->hyb_s1, (void*)p->hyb_tabs, (void*)p->hyb_g, (void*)p->hyb_mx, p->p1g_tab})
     if (q) cudaFree(q);
   if (p->wbuf) cudaFree(p->wbuf);
   for (auto& kv : p->tables) {
@@ -531,6 +531,10 @@ srk_status srk_plan_set_schedule(srk_plan p, srk_schedule sch) {
       p->hyb_s1_bytes = bytes;
     }
     if (!p->hyb_mx) SRK_CUDA(cudaMalloc(reinterpret_cast<void**>(&p->hyb_mx), (size_t)p->chunk * sizeof(unsigned int)));
+    if (!p->p1g_tab) {
+      SRK_CUDA(cudaMalloc(&p->p1g_tab, tensor_rows_p1g_tab_bytes()));
+      SRK_TRY(tensor_rows_p1g_tables(p, nullptr));
+    }
     p->schedule = sch;
     SRK_TRY(refresh_direct(p, nullptr));
     SRK_CUDA(cudaStreamSynchronize(nullptr));

@@ -1,10 +1,11 @@
-"""The tensor-core row pass (SRK_SCHEDULE_TENSOR_ROWS, FP16/BF16 storage at
-tile 512): after the column FFT the convolution along x runs per frequency
-row as a banded complex matrix product on tcgen05 with FP16 column spectra.
+"""The tensor-core row schedule (SRK_SCHEDULE_TENSOR_ROWS, FP16/BF16 storage
+at tile 512): after the column transform (a DFT on the tensor cores where
+its TMA boxes apply, else the column FFT) the convolution along x runs per
+frequency row as a banded complex matrix product on tcgen05 with FP16
+column spectra.  It serves the pair ops (training forward, OaS forward,
+VJP); the tangent and tangent-adjoint run the FFT schedule on such a plan.
 Checked against the FP64 oracle (storage tolerance rel 1e-2 / abs 1e-3)
-and against the FFT row pass on the same inputs, for the training forward
-(one chunk and a ring of chunks), the OaS forward with its ux / uy outputs,
-the tangent, the VJP and the tangent-adjoint."""
+and against the FFT row pass on the same inputs."""
 import numpy as np
 import pytest
 
@@ -122,14 +123,17 @@ def test_tensor_rows_mixed_amplitudes_ring(torch_cuda):
 
 
 @pytest.mark.parametrize("dt", ["f16", "bf16"])
-def test_tensor_rows_single_image_ops(torch_cuda, dt):
-    """N = 4096, KW = 61 (81 forward tiles of 512): the OaS forward with
-    ux / uy, the tangent and the tangent-adjoint on oracle windows; the VJP
-    against the same VJP on the FFT row pass."""
+@pytest.mark.parametrize("N,KW", [(4096, 61), (1024, 121)])
+def test_tensor_rows_single_image_ops(torch_cuda, dt, N, KW):
+    """One image of several tiles of 512: the OaS forward with ux / uy, the
+    tangent and the tangent-adjoint (the FFT schedule on this plan) on oracle
+    windows; the VJP against the same VJP on the FFT row pass.  At N = 4096,
+    KW = 61 the tile stride (452) is not a multiple of 8 and the column FFT
+    runs; at N = 1024, KW = 121 (stride 392) the column DFT on the tensor
+    cores."""
     torch = torch_cuda
     sdt, tname = DT[dt]
     tdt = getattr(torch, tname)
-    N, KW = 4096, 61
     e = (KW - 1) // 2
     W = N - 2 * e
     Kx, Ky = kernel(KW)
