@@ -70,15 +70,17 @@ typedef enum srk_schedule {
   SRK_SCHEDULE_TENSOR_ROWS = 3
 } srk_schedule;
 /* SRK_SCHEDULE_TENSOR_ROWS (FP16/BF16 storage plans at tile 512, erosion
- * 1..64): the three-pass schedule with its row pass on the tensor cores —
- * after the column FFT, the convolution along x is applied per frequency
- * row as a banded complex matrix product (tcgen05.mma, FP16 operands:
- * the column spectra are stored as FP16, FP32 accumulation) instead of the
- * row FFT, spectral product and inverse row FFT.  Used by the forward-type
- * operators (training forward, forward, tangent, VJP and tangent-adjoint
- * dL/df parts); the adjoint-type pass keeps the FFT row pass.  The plan
- * allocates the FP16 spectra planes (1 MB per work tile of its scratch)
- * when the schedule is set. */
+ * 1..64): the three-pass schedule with its first two passes on the tensor
+ * cores — the column transform as a DFT (tcgen05.mma against cos / -sin
+ * tables; the column FFT where the tile origins are not on 8-row boundaries
+ * or N % 8 != 0) and the convolution along x per frequency row as a banded
+ * complex matrix product instead of the row FFT, spectral product and
+ * inverse row FFT (FP16 operands: the column spectra are stored as FP16,
+ * FP32 accumulation).  Used by the pair operators (training forward,
+ * forward, the VJP's forward part); the tangent, the tangent-adjoint and
+ * the adjoint-type pass run the three-pass FFT schedule on such a plan.
+ * The plan allocates the FP16 spectra planes (1 MB per work tile of its
+ * scratch) and the DFT tables (512 KB) when the schedule is set. */
 /* SRK_SCHEDULE_DIRECT: the training forward and srk_forward run as a direct
  * convolution on the tensor cores (tcgen05.mma, FP32 accumulation; FP16/BF16
  * storage in one pass, FP32 storage in three passes over an exact FP16
