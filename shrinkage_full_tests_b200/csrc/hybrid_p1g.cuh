@@ -40,15 +40,32 @@ constexpr int M = 512;
 constexpr int KR = 128;                  // ky rows per item (TMEM lanes)
 constexpr int XB = 64;                   // columns x per item and source
 constexpr int NA = M / 64;               // K atoms of 64 rows y
-constexpr int NSG = 3;                   // ring stages (one atom each)
-constexpr int kEpi = 4;                  // epilogue warps, one per TMEM lane quarter
+// Staging buffers (1: one pair of blocks, each item waits for the previous
+// item's stores to read it; 2: one pair per item parity, with a ring of 2
+// stages to fit), epilogue warps (4 or 8: one or two per TMEM lane quarter).
+// Measured (B = 5000 FP16 step): 1 / 4 8.50 ms, 1 / 8 8.50 ms, 2 / 8 8.81 ms
+// (two stages starve the MMAs).
+#ifndef SRK_P1G_STAGING
+#define SRK_P1G_STAGING 1
+#endif
+#ifndef SRK_P1G_EPI
+#define SRK_P1G_EPI 4
+#endif
+constexpr int kStagings = SRK_P1G_STAGING;
+constexpr int NSG = kStagings == 2 ? 2 : 3;  // ring stages (one atom each)
+constexpr int kEpi = SRK_P1G_EPI;
+static_assert((kEpi == 4 || kEpi == 8) && XB == 64 && (kStagings == 1 || kStagings == 2), "configuration");
+constexpr int kColsW = XB / (kEpi / 4);  // columns of each source per epilogue warp
 constexpr int kThreadsG = 32 * (kEpi + 2);
 constexpr int kLoadWarp = kEpi, kMmaWarp = kEpi + 1;
 constexpr uint32_t kTabBox = KR * 128;   // 128 table rows x 64 y, 16 KB
 constexpr uint32_t kSrcBox = XB * 128;   // 64 columns x 64 y, 8 KB
 constexpr uint32_t kStage = 2 * kTabBox + 2 * kSrcBox;
 constexpr uint32_t kStaging = 256 * 128;  // 256 plane rows x 64 FP16 columns
-__host__ __device__ constexpr size_t smem_bytes() { return 1024 + (size_t)NSG * kStage + 2 * (size_t)kStaging; }
+// barriers | NSG stages | staging (per buffer: rows ky, rows M - ky)
+__host__ __device__ constexpr size_t smem_bytes() {
+  return 1024 + (size_t)NSG * kStage + 2 * (size_t)kStagings * kStaging;
+}
 
 struct Args {
   __half* planes;            // the chunk's planes [2M][c][M] (the Nyquist row is stored directly)
@@ -103,8 +120,7 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   volatile int* go = abort_flag + 1;                   // the epilogue's per-item decision
   unsigned char* St = smem + 1024;                     // NSG stages: C | S | source a | source b
-  unsigned char* Sk = St + (size_t)NSG * kStage;       // staging: rows ky (256 plane rows)
-  unsigned char* Sm = Sk + kStaging;                   // staging: rows M - ky
+  unsigned char* Sg = St + (size_t)NSG * kStage;       // staging [item parity][rows ky | rows M - ky]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int items = a.c * (M / XB) * 2;
   const unsigned long long lim = a.spin_limit;
@@ -202,10 +218,11 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
     }
     __syncwarp();
   } else {
-    // epilogue warp: TMEM lanes 32 warp .. + 31 = rows r of the ky block
-    const int r = warp * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-    const uint32_t sk = smem_u32(Sk), sm = smem_u32(Sm);
+    // epilogue warp: TMEM lanes 32 (warp % 4) .. + 31 = rows r of the ky
+    // block, columns kColsW (warp / 4) .. of each source
+    const int quarter = warp & 3, colh = warp >> 2;
+    const int r = quarter * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
     const uint32_t rk = 2 * r, rm = 2 * (KR - 1 - r);  // staging rows of ky and of M - ky (part 0; part 1 = +1)
     for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
       const int t = k & 1;
@@ -213,9 +230,12 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
       decode(item, wl, xb, kt);
       // One thread decides for all epilogue warps, so that they leave together
       // (they meet at named barriers): the accumulators are complete and the
-      // staging blocks free (the previous item's stores have read them).
+      // staging blocks free (the stores that last used them have read them).
       if (threadIdx.x == 0) {
-        bulk_wait_read();
+        if (kStagings == 2)
+          bulk_wait_read_but1();  // item k - 2 used this parity's buffer
+        else
+          bulk_wait_read();
         const bool w = mbar_wait(tfull + t, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
         *go = w ? 1 : 0;
         if (!w) {
@@ -229,9 +249,12 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
       tc_fence_after();
       const bool nyq = kt == 0 && r == 0;  // rows 0 and M/2 instead of 0 and its mirror
       const uint32_t tb = trow + (uint32_t)t * 256;
+      unsigned char* Sk = Sg + (size_t)(kStagings == 2 ? (k & 1) : 0) * 2 * kStaging;
+      unsigned char* Sm = Sk + kStaging;
+      const uint32_t sk = smem_u32(Sk), sm = smem_u32(Sm);
       float m = 0.f;
 #pragma unroll 1
-      for (int n0 = 0; n0 < XB; n0 += 16) {
+      for (int n0 = colh * kColsW; n0 < colh * kColsW + kColsW; n0 += 16) {
         float ar[16], br[16], ai[16], bi[16];
         tmem_ld16(tb + (uint32_t)n0, ar);              // Re A (source a), columns n0 ..
         tmem_ld16(tb + XB + (uint32_t)n0, br);         // Re B (source b)
