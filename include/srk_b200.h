@@ -80,7 +80,7 @@ typedef enum srk_schedule {
  * forward, the VJP's forward part); the tangent, the tangent-adjoint and
  * the adjoint-type pass run the three-pass FFT schedule on such a plan.
  * The plan allocates the FP16 spectra planes (1 MB per work tile of its
- * scratch) and the DFT tables (512 KB) when the schedule is set. */
+ * scratch) and the DFT tables (256 KB) when the schedule is set. */
 /* SRK_SCHEDULE_DIRECT: the training forward and srk_forward run as a direct
  * convolution on the tensor cores (tcgen05.mma, FP32 accumulation; FP16/BF16
  * storage in one pass, FP32 storage in three passes over an exact FP16

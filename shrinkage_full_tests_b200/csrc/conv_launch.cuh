@@ -53,8 +53,8 @@ srk_status launch_tensor_rows(srk_plan_s* p, const OpArgs& a, const Geom& g, int
     SRK_TRY(tensor_rows_plane_map(planes, c, kP1hCols, 1, kP1hBox, &pmap));
     SRK_CUDA(cudaMemsetAsync(max_of(k), 0, (size_t)c * sizeof(unsigned int), st));
     if (dft) {
-      CUtensorMap pmapg;  // 256 plane rows x 64 columns, 128-byte swizzle
-      SRK_TRY(tensor_rows_plane_map(planes, c, p1g::XB, 1, 256, &pmapg, true));
+      CUtensorMap pmapg;  // 128 ky rows of one parity x 2 parts x 64 columns, 128-byte swizzle
+      SRK_TRY(tensor_rows_p1g_store_map(planes, c, &pmapg));
       p1g::Args ga;
       ga.planes = planes;
       ga.zmax = max_of(k);

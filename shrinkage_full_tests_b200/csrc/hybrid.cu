@@ -410,10 +410,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn_h() {
 }
 }  // namespace
 
-// The column-DFT tables of k_p1g (C and S rows, 512 KB), in the plan's storage type.
-size_t tensor_rows_p1g_tab_bytes() { return (size_t)2 * (p1g::M / 2) * p1g::M * 2; }
+// The column-DFT tables of k_p1g (C and S rows of both parities over y < M/2,
+// 256 KB), in the plan's storage type.
+size_t tensor_rows_p1g_tab_bytes() { return (size_t)2 * (p1g::M / 2) * (p1g::M / 2) * 2; }
 srk_status tensor_rows_p1g_tables(srk_plan_s* p, cudaStream_t s) {
-  const int n = 2 * (p1g::M / 2) * p1g::M;
+  const int n = 2 * (p1g::M / 2) * (p1g::M / 2);
   if (p->dtype == SRK_BF16)
     p1g::k_p1g_tables<__nv_bfloat16><<<(n + 255) / 256, 256, 0, s>>>(static_cast<__nv_bfloat16*>(p->p1g_tab));
   else
@@ -431,8 +432,8 @@ srk_status tensor_rows_p1g_maps(const srk_plan_s* p, const void* img, int N, int
   const CUtensorMapDataType dt = p->dtype == SRK_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
   {
     std::memset(tmap, 0, sizeof(*tmap));
-    const cuuint64_t dims[2] = {(cuuint64_t)p1g::M, (cuuint64_t)p1g::M};
-    const cuuint64_t strides[1] = {(cuuint64_t)p1g::M * 2};
+    const cuuint64_t dims[2] = {(cuuint64_t)p1g::M / 2, (cuuint64_t)p1g::M};
+    const cuuint64_t strides[1] = {(cuuint64_t)p1g::M / 2 * 2};
     const cuuint32_t box[2] = {64, (cuuint32_t)p1g::KR};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult r = enc(tmap, dt, 2, p->p1g_tab, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -452,6 +453,23 @@ srk_status tensor_rows_p1g_maps(const srk_plan_s* p, const void* img, int N, int
     if (r != CUDA_SUCCESS) return fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled (images) failed (%d)", (int)r);
   }
   return SRK_OK;
+}
+
+// The planes [2M][c][M] as [ky][part][wl][x] for k_p1g's stores: box {64 x,
+// 1 work tile, 2 parts, 256 ky traversed with stride 2} = 128 rows of one ky
+// parity, 128-byte swizzle.
+srk_status tensor_rows_p1g_store_map(const __half* planes, int c, CUtensorMap* out) {
+  auto enc = encode_fn_h();
+  if (!enc) return fail(SRK_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is unavailable");
+  std::memset(out, 0, sizeof(*out));
+  const cuuint64_t dims[4] = {(cuuint64_t)p1g::M, (cuuint64_t)c, 2, (cuuint64_t)p1g::M};
+  const cuuint64_t strides[3] = {(cuuint64_t)p1g::M * 2, (cuuint64_t)c * p1g::M * 2, (cuuint64_t)2 * c * p1g::M * 2};
+  const cuuint32_t box[4] = {(cuuint32_t)p1g::XB, 1, 2, 2 * p1g::KR};
+  const cuuint32_t estr[4] = {1, 1, 1, 2};
+  const CUresult r = enc(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, const_cast<__half*>(planes), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? SRK_OK : fail(SRK_ERR_CUDA, "cuTensorMapEncodeTiled (plane stores) failed (%d)", (int)r);
 }
 
 srk_status tensor_rows_plane_map(const __half* planes, int c, unsigned box_x, unsigned box_w, unsigned box_p,

@@ -8,20 +8,27 @@
 //   Z[ky]     = (Re A - Im B) + i (Im A + Re B)
 //   Z[M - ky] = (Re A + Im B) + i (Re B - Im A),
 // so ky = 0 .. M/2 - 1 give every row but the Nyquist row M/2.  Per item
-// (128 ky rows, 64 columns x of both sources) two real GEMMs with K = y:
-//   Dr = C  [a | b],   C[ky][y]  = cos(2 pi ky y / M)
-//   Di = S  [a | b],   S[ky][y]  = -sin(2 pi ky y / M)
-// (N = 128: 64 columns of a, then the same 64 of b).  The row ky = 0 of S is
-// zero; the table holds the Nyquist row (-1)^y there instead, so that lane
-// also yields Re A[M/2], Re B[M/2] (Im of both is zero at ky = 0 and M/2).
-// The tables and images are FP16 (or BF16 for BF16 storage) operands with
-// FP32 accumulation: the planes are FP16 anyway.
+// (128 ky rows of one parity, 64 columns x of both sources) two real GEMMs
+// with K = y:
+//   Dr = C [a | b],   C[ky][y] = cos(2 pi ky y / M)
+//   Di = S [a | b],   S[ky][y] = -sin(2 pi ky y / M)
+// (N = 128: 64 columns of a, then the same 64 of b).  Items take the even
+// or the odd ky < M/2: C and S at y + M/2 are (-1)^ky times their values
+// at y, so the tables cover y < M/2 only and each table atom multiplies the
+// image atoms at y and at y + M/2 (the second with the instruction's
+// negate-A bit for odd ky) — half the table bytes per unit of work.  The
+// row ky = 0 of S is zero; the table holds the Nyquist row (-1)^y there
+// instead (even at y + M/2 too), so that lane also yields Re A[M/2] and
+// Re B[M/2] (Im of both is zero at ky = 0 and M/2).  The tables and images
+// are FP16 (or BF16 for BF16 storage) operands with FP32 accumulation: the
+// planes are FP16 anyway.
 //
 // Data movement: the tables (128 ky x 64 y boxes) and the source tiles
 // (64 x x 64 y boxes, the images' own column-major layout is the K-major
 // operand) by TMA with the 128-byte swizzle through a ring of stages; the
-// planes leave through shared memory by TMA stores of 256 plane rows x 64
-// columns (128-byte rows), the Nyquist row by the threads.
+// planes leave through shared memory by 4-D TMA stores whose ky dimension
+// steps by 2 (128 rows of one parity, both parts, 64 columns: 128-byte
+// rows), the Nyquist row by the threads.
 // Used with tile origins on 8-row boundaries (TMA's innermost coordinate):
 // one tile per image, or a tile stride that is a multiple of 8.  The tables'
 // FP16 rounding adds an error relative to the larger image of the pair, of
@@ -39,33 +46,18 @@ using namespace srk::tc;
 constexpr int M = 512;
 constexpr int KR = 128;                  // ky rows per item (TMEM lanes)
 constexpr int XB = 64;                   // columns x per item and source
-constexpr int NA = M / 64;               // K atoms of 64 rows y
-// Staging buffers (1: one pair of blocks, each item waits for the previous
-// item's stores to read it; 2: one pair per item parity, with a ring of 2
-// stages to fit), epilogue warps (4 or 8: one or two per TMEM lane quarter).
-// Measured (B = 5000 FP16 step): 1 / 4 8.50 ms, 1 / 8 8.50 ms, 2 / 8 8.81 ms
-// (two stages starve the MMAs).
-#ifndef SRK_P1G_STAGING
-#define SRK_P1G_STAGING 1
-#endif
-#ifndef SRK_P1G_EPI
-#define SRK_P1G_EPI 4
-#endif
-constexpr int kStagings = SRK_P1G_STAGING;
-constexpr int NSG = kStagings == 2 ? 2 : 3;  // ring stages (one atom each)
-constexpr int kEpi = SRK_P1G_EPI;
-static_assert((kEpi == 4 || kEpi == 8) && XB == 64 && (kStagings == 1 || kStagings == 2), "configuration");
-constexpr int kColsW = XB / (kEpi / 4);  // columns of each source per epilogue warp
+constexpr int NA = M / 2 / 64;           // table atoms of 64 rows y (each with the image atoms y and y + M/2)
+constexpr int NSG = 3;                   // ring stages (one table atom each)
+constexpr int kEpi = 4;                  // epilogue warps, one per TMEM lane quarter
 constexpr int kThreadsG = 32 * (kEpi + 2);
 constexpr int kLoadWarp = kEpi, kMmaWarp = kEpi + 1;
 constexpr uint32_t kTabBox = KR * 128;   // 128 table rows x 64 y, 16 KB
 constexpr uint32_t kSrcBox = XB * 128;   // 64 columns x 64 y, 8 KB
-constexpr uint32_t kStage = 2 * kTabBox + 2 * kSrcBox;
-constexpr uint32_t kStaging = 256 * 128;  // 256 plane rows x 64 FP16 columns
-// barriers | NSG stages | staging (per buffer: rows ky, rows M - ky)
-__host__ __device__ constexpr size_t smem_bytes() {
-  return 1024 + (size_t)NSG * kStage + 2 * (size_t)kStagings * kStaging;
-}
+constexpr uint32_t kSrcAtom = 2 * kSrcBox;                 // both sources: the MMA's 128 B operand rows
+constexpr uint32_t kStage = 2 * kTabBox + 2 * kSrcAtom;    // C | S | images at y | images at y + M/2
+constexpr uint32_t kStaging = 256 * 128;  // 128 ky rows x 2 parts x 64 FP16 columns
+// barriers | NSG stages | staging (rows ky, then rows M - ky, of one item)
+__host__ __device__ constexpr size_t smem_bytes() { return 1024 + (size_t)NSG * kStage + kStaging; }
 
 struct Args {
   __half* planes;            // the chunk's planes [2M][c][M] (the Nyquist row is stored directly)
@@ -77,13 +69,14 @@ struct Args {
   int nimg;                  // images in the image map (a coordinate there reads zeros)
 };
 
-// C and S tables (rows part * 256 + ky, ky < 256; columns y < M), in the
-// storage type's 16-bit format.
+// C and S tables: rows part * 256 + p * 128 + r for ky = p + 2 r (parity p),
+// columns y < M/2, in the storage type's 16-bit format.
 template <typename T>
 __global__ void k_p1g_tables(T* __restrict__ tab) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= 2 * (M / 2) * M) return;
-  const int y = idx % M, row = idx / M, part = row / (M / 2), ky = row % (M / 2);
+  if (idx >= 2 * (M / 2) * (M / 2)) return;
+  const int y = idx % (M / 2), row = idx / (M / 2), part = row / (M / 2);
+  const int par = (row % (M / 2)) / KR, r = row % KR, ky = par + 2 * r;
   const int m = (ky * y) % M;
   double s, c;
   sincospi(2.0 * m / M, &s, &c);
@@ -103,8 +96,8 @@ __device__ __forceinline__ uint32_t pack_h2(float x, float y) {
   return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// Persistent, one CTA per SM; an item is (work tile wl, column block xb,
-// ky block kt) with kt fastest (both ky blocks read the same source boxes).
+// Persistent, one CTA per SM; an item is (work tile wl, column block xb, ky
+// parity kt) with kt fastest (both parities read the same source boxes).
 //   full[s] / empty[s]: ring stage s loaded (TMA bytes) / read by the MMAs (commit)
 //   tfull[t] / tempty[t]: accumulator set t complete (commit) / drained (epilogue warps)
 template <typename T>
@@ -119,8 +112,8 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   volatile int* go = abort_flag + 1;                   // the epilogue's per-item decision
-  unsigned char* St = smem + 1024;                     // NSG stages: C | S | source a | source b
-  unsigned char* Sg = St + (size_t)NSG * kStage;       // staging [item parity][rows ky | rows M - ky]
+  unsigned char* St = smem + 1024;                     // NSG stages: C | S | images at y | images at y + M/2
+  unsigned char* Sk = St + (size_t)NSG * kStage;       // staging: rows ky, then rows M - ky
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int items = a.c * (M / XB) * 2;
   const unsigned long long lim = a.spin_limit;
@@ -172,10 +165,14 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
           }
           unsigned char* S = St + (size_t)st * kStage;
           mbar_expect_tx(full + st, kStage);
-          tma_load_2d(S, &tmap, 64 * at, kt * KR, full + st);                        // C rows
+          tma_load_2d(S, &tmap, 64 * at, kt * KR, full + st);                        // C rows of parity kt
           tma_load_2d(S + kTabBox, &tmap, 64 * at, M / 2 + kt * KR, full + st);      // S rows
-          tma_load_3d(S + 2 * kTabBox, &smap, t0.y0 + 64 * at, t0.x0 + XB * xb, i0, full + st);
-          tma_load_3d(S + 2 * kTabBox + kSrcBox, &smap, t1.y0 + 64 * at, t1.x0 + XB * xb, i1, full + st);
+          for (int h = 0; h < 2; ++h) {                                              // y and y + M/2
+            unsigned char* D = S + 2 * kTabBox + h * kSrcAtom;
+            const int y = 64 * at + h * (M / 2);
+            tma_load_3d(D, &smap, t0.y0 + y, t0.x0 + XB * xb, i0, full + st);
+            tma_load_3d(D + kSrcBox, &smap, t1.y0 + y, t1.x0 + XB * xb, i1, full + st);
+          }
         }
       }
       for (long long r = q > NSG ? q - NSG : 0; r < q; ++r) mbar_wait(full + (int)(r % NSG), (unsigned)((r / NSG) & 1), lim);
@@ -185,10 +182,12 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
     if (lane == 0) {
       constexpr int kFmt = std::is_same<T, __nv_bfloat16>::value ? 1 : 0;
       const uint32_t id = idesc_f16(kFmt, KR, 2 * XB);
+      const uint32_t idn = id | (1u << 13);  // negate A: the odd rows' tables at y + M/2
       long long q = 0;
       bool ok = true;
       for (int k = 0, item = blockIdx.x; item < items && ok; ++k, item += gridDim.x) {
         const int t = k & 1;
+        const uint32_t idh = (item & 1) ? idn : id;  // parity kt = item & 1
         if (k >= 2 && !mbar_wait(tempty + t, (unsigned)((k / 2 - 1) & 1), lim)) ok = false;
         const uint32_t dr = tmem + (uint32_t)t * 256, di = dr + 128;
         for (int at = 0; at < NA && ok; ++at, ++q) {
@@ -203,9 +202,12 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
           for (int kk = 0; kk < 4; ++kk) {
             const uint64_t dc = sdesc_sw128(base + (uint32_t)kk * 32);
             const uint64_t ds = sdesc_sw128(base + kTabBox + (uint32_t)kk * 32);
-            const uint64_t db = sdesc_sw128(base + 2 * kTabBox + (uint32_t)kk * 32);
-            mma_f16(dr, dc, db, id, (at | kk) != 0);
-            mma_f16(di, ds, db, id, (at | kk) != 0);
+            const uint64_t dlo = sdesc_sw128(base + 2 * kTabBox + (uint32_t)kk * 32);
+            const uint64_t dhi = sdesc_sw128(base + 2 * kTabBox + kSrcAtom + (uint32_t)kk * 32);
+            mma_f16(dr, dc, dlo, id, (at | kk) != 0);
+            mma_f16(dr, dc, dhi, idh, true);
+            mma_f16(di, ds, dlo, id, (at | kk) != 0);
+            mma_f16(di, ds, dhi, idh, true);
           }
           mma_commit(empty + st);
         }
@@ -218,24 +220,19 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
     }
     __syncwarp();
   } else {
-    // epilogue warp: TMEM lanes 32 (warp % 4) .. + 31 = rows r of the ky
-    // block, columns kColsW (warp / 4) .. of each source
-    const int quarter = warp & 3, colh = warp >> 2;
-    const int r = quarter * 32 + lane;
-    const uint32_t trow = tmem + ((uint32_t)(quarter * 32) << 16);
-    const uint32_t rk = 2 * r, rm = 2 * (KR - 1 - r);  // staging rows of ky and of M - ky (part 0; part 1 = +1)
+    // epilogue warp: TMEM lanes 32 warp .. + 31 = rows r of the item, ky = kt + 2 r
+    const int r = warp * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t sk = smem_u32(Sk);
     for (int k = 0, item = blockIdx.x; item < items; ++k, item += gridDim.x) {
       const int t = k & 1;
       int wl, xb, kt;
       decode(item, wl, xb, kt);
       // One thread decides for all epilogue warps, so that they leave together
       // (they meet at named barriers): the accumulators are complete and the
-      // staging blocks free (the stores that last used them have read them).
+      // staging block free (the previous item's stores have read it).
       if (threadIdx.x == 0) {
-        if (kStagings == 2)
-          bulk_wait_read_but1();  // item k - 2 used this parity's buffer
-        else
-          bulk_wait_read();
+        bulk_wait_read();
         const bool w = mbar_wait(tfull + t, (unsigned)((k / 2) & 1), lim) && !*abort_flag;
         *go = w ? 1 : 0;
         if (!w) {
@@ -249,56 +246,69 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
       tc_fence_after();
       const bool nyq = kt == 0 && r == 0;  // rows 0 and M/2 instead of 0 and its mirror
       const uint32_t tb = trow + (uint32_t)t * 256;
-      unsigned char* Sk = Sg + (size_t)(kStagings == 2 ? (k & 1) : 0) * 2 * kStaging;
-      unsigned char* Sm = Sk + kStaging;
-      const uint32_t sk = smem_u32(Sk), sm = smem_u32(Sm);
       float m = 0.f;
+      // pass 0: rows ky (staging row 2 r + part) -> store from ky = kt;
+      // pass 1: rows M - ky (staging row 2 (127 - r) + part) -> store from
+      // ky = M/2 + 2 - kt (the row past M, r = 0 at kt = 0, is dropped) and
+      // the Nyquist row by the threads
 #pragma unroll 1
-      for (int n0 = colh * kColsW; n0 < colh * kColsW + kColsW; n0 += 16) {
-        float ar[16], br[16], ai[16], bi[16];
-        tmem_ld16(tb + (uint32_t)n0, ar);              // Re A (source a), columns n0 ..
-        tmem_ld16(tb + XB + (uint32_t)n0, br);         // Re B (source b)
-        tmem_ld16(tb + 128 + (uint32_t)n0, ai);        // Im A
-        tmem_ld16(tb + 128 + XB + (uint32_t)n0, bi);   // Im B
-        tmem_wait_ld();
-        uint32_t kre[8], kim[8], mre[8], mim[8];
+      for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+          if (threadIdx.x == 0) bulk_wait_read();  // the rows-ky store has read the staging block
+          named_sync(1, 32 * kEpi);
+        }
+        const uint32_t row = pass == 0 ? 2 * r : 2 * (KR - 1 - r);
+#pragma unroll 1
+        for (int n0 = 0; n0 < XB; n0 += 16) {
+          float ar[16], br[16], ai[16], bi[16];
+          tmem_ld16(tb + (uint32_t)n0, ar);              // Re A (source a), columns n0 ..
+          tmem_ld16(tb + XB + (uint32_t)n0, br);         // Re B (source b)
+          tmem_ld16(tb + 128 + (uint32_t)n0, ai);        // Im A
+          tmem_ld16(tb + 128 + XB + (uint32_t)n0, bi);   // Im B
+          tmem_wait_ld();
+          uint32_t vre[8], vim[8];
 #pragma unroll
-        for (int j = 0; j < 16; j += 2) {
-          float kr[2], ki[2], mr[2], mi[2];
+          for (int j = 0; j < 16; j += 2) {
+            float zr[2], zi[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const float ra = ar[j + h], rb = br[j + h], ia = ai[j + h], ib = bi[j + h];
+              if (pass == 0) {
+                zr[h] = nyq ? ra : ra - ib;  // Z[ky]
+                zi[h] = nyq ? rb : ia + rb;
+                // bounds every |component| of Z[ky] and Z[M - ky] (the Nyquist row too)
+                m = fmaxf(m, fmaxf(fabsf(ra) + fabsf(ib), fabsf(ia) + fabsf(rb)));
+              } else {
+                zr[h] = nyq ? ia : ra + ib;  // Z[M - ky]; the Nyquist row: Re A[M/2], Re B[M/2]
+                zi[h] = nyq ? ib : rb - ia;
+              }
+            }
+            vre[j / 2] = pack_h2(zr[0], zr[1]);
+            vim[j / 2] = pack_h2(zi[0], zi[1]);
+          }
+          const uint32_t c0 = (uint32_t)n0 / 8;  // first 16-byte chunk of these 16 columns
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const float ra = ar[j + h], rb = br[j + h], ia = ai[j + h], ib = bi[j + h];
-            kr[h] = nyq ? ra : ra - ib;
-            ki[h] = nyq ? rb : ia + rb;
-            mr[h] = nyq ? ia : ra + ib;  // the Nyquist row: Re A[M/2], Re B[M/2]
-            mi[h] = nyq ? ib : rb - ia;
-            m = fmaxf(m, fmaxf(fmaxf(fabsf(kr[h]), fabsf(ki[h])), fmaxf(fabsf(mr[h]), fabsf(mi[h]))));
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sk + sw128(row, c0 + h)), "r"(vre[4 * h]),
+                         "r"(vre[4 * h + 1]), "r"(vre[4 * h + 2]), "r"(vre[4 * h + 3]) : "memory");
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sk + sw128(row + 1, c0 + h)),
+                         "r"(vim[4 * h]), "r"(vim[4 * h + 1]), "r"(vim[4 * h + 2]), "r"(vim[4 * h + 3]) : "memory");
           }
-          kre[j / 2] = pack_h2(kr[0], kr[1]);
-          kim[j / 2] = pack_h2(ki[0], ki[1]);
-          mre[j / 2] = pack_h2(mr[0], mr[1]);
-          mim[j / 2] = pack_h2(mi[0], mi[1]);
+          if (pass == 1 && nyq) {
+            // planes M (re) and M + 1 (im) of work tile wl, columns XB xb + n0 ..
+            uint4* pr = reinterpret_cast<uint4*>(a.planes + ((size_t)M * a.c + wl) * M + XB * xb + n0);
+            uint4* pi = reinterpret_cast<uint4*>(a.planes + ((size_t)(M + 1) * a.c + wl) * M + XB * xb + n0);
+            pr[0] = make_uint4(vre[0], vre[1], vre[2], vre[3]);
+            pr[1] = make_uint4(vre[4], vre[5], vre[6], vre[7]);
+            pi[0] = make_uint4(vim[0], vim[1], vim[2], vim[3]);
+            pi[1] = make_uint4(vim[4], vim[5], vim[6], vim[7]);
+          }
         }
-        const uint32_t c0 = (uint32_t)n0 / 8;  // first 16-byte chunk of these 16 columns
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sk + sw128(rk, c0 + h)), "r"(kre[4 * h]),
-                       "r"(kre[4 * h + 1]), "r"(kre[4 * h + 2]), "r"(kre[4 * h + 3]) : "memory");
-          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sk + sw128(rk + 1, c0 + h)), "r"(kim[4 * h]),
-                       "r"(kim[4 * h + 1]), "r"(kim[4 * h + 2]), "r"(kim[4 * h + 3]) : "memory");
-          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sm + sw128(rm, c0 + h)), "r"(mre[4 * h]),
-                       "r"(mre[4 * h + 1]), "r"(mre[4 * h + 2]), "r"(mre[4 * h + 3]) : "memory");
-          asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sm + sw128(rm + 1, c0 + h)), "r"(mim[4 * h]),
-                       "r"(mim[4 * h + 1]), "r"(mim[4 * h + 2]), "r"(mim[4 * h + 3]) : "memory");
-        }
-        if (nyq) {
-          // planes M (re) and M + 1 (im) of work tile wl, columns XB xb + n0 ..
-          uint4* pr = reinterpret_cast<uint4*>(a.planes + ((size_t)M * a.c + wl) * M + XB * xb + n0);
-          uint4* pi = reinterpret_cast<uint4*>(a.planes + ((size_t)(M + 1) * a.c + wl) * M + XB * xb + n0);
-          pr[0] = make_uint4(mre[0], mre[1], mre[2], mre[3]);
-          pr[1] = make_uint4(mre[4], mre[5], mre[6], mre[7]);
-          pi[0] = make_uint4(mim[0], mim[1], mim[2], mim[3]);
-          pi[1] = make_uint4(mim[4], mim[5], mim[6], mim[7]);
+        fence_async_smem();
+        named_sync(1, 32 * kEpi);
+        if (threadIdx.x == 0) {
+          tma_store_4d(&pmap, XB * xb, wl, 0, pass == 0 ? kt : M / 2 + 2 - kt, Sk);
+          bulk_commit();
         }
       }
       // accumulators t are free for item k + 2
@@ -308,14 +318,6 @@ k_p1g(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensor
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
       if (lane == 0 && m > 0.f) atomicMax(a.zmax + wl, __float_as_uint(m));
-      // staging complete: two stores of 256 plane rows x 64 columns (rows past the planes are dropped)
-      fence_async_smem();
-      named_sync(1, 32 * kEpi);
-      if (threadIdx.x == 0) {
-        tma_store_3d(&pmap, XB * xb, wl, 2 * kt * KR, Sk);
-        tma_store_3d(&pmap, XB * xb, wl, 2 * (M - kt * KR - (KR - 1)), Sm);
-        bulk_commit();
-      }
     }
     if (threadIdx.x == 0) bulk_wait_all();
   }

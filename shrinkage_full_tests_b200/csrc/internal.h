@@ -166,6 +166,7 @@ srk_status tensor_rows_build_tables(srk_plan_s* p, cudaStream_t s);
 srk_status tensor_rows_p2(srk_plan_s* p, const __half* planes, const unsigned int* mx, int c, float2* scratch,
                           size_t per, size_t s1, int S, int P, cudaStream_t s);
 size_t tensor_rows_p1g_tab_bytes();
+srk_status tensor_rows_p1g_store_map(const __half* planes, int c, CUtensorMap* out);
 srk_status tensor_rows_p1g_tables(srk_plan_s* p, cudaStream_t s);
 srk_status tensor_rows_p1g_maps(const srk_plan_s* p, const void* img, int N, int nimg, CUtensorMap* tmap,
                                 CUtensorMap* smap);
