@@ -420,8 +420,8 @@ def half_storage_rate(torch, srk, E32, GX, GY, N, W, e, dx, B, steps=20):
     alg = B * (N * N + W * W) * 2
     info = plan.info()
     sched = ["persistent", "three_pass", "direct", "tensor_rows"][info["schedule"]]
-    arith = ("f32 FFTs, f16 x f16 -> f32 row convolution on the tensor cores" if sched == "tensor_rows"
-             else "f32 arithmetic")
+    arith = ("f16 x f16 -> f32 column DFT and row convolution on the tensor cores, f32 inverse column FFT"
+             if sched == "tensor_rows" else "f32 arithmetic")
     out = {"value": B / (ms * 1e-3), "unit": "img/s", "ms_per_step": ms, "dtype": "f16 storage, " + arith,
            "hbm_frac": alg / (ms * 1e-3) / 1e9 / peak, "tile_M": info["tile_M"], "schedule": sched}
     del E, R, plan
